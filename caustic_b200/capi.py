@@ -1,0 +1,276 @@
+"""ctypes binding of libcausticot.so (include/causticot.h).
+
+The shared library is the product: every call here goes to the sm_100a CUDA
+path.  There is no CPU fallback; if the library is missing or no GPU is
+visible the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libcausticot.so")
+
+COT_OK = 0
+COT_EINVAL = -1
+COT_ECUDA = -2
+COT_ENOPROBLEM = -3
+COT_ECAPACITY = -4
+COT_ERING = -5
+COT_ENOTCONV = -6
+COT_ETIMEOUT = -7
+COT_ENOMEM = -8
+
+COT_MEM_HOST = 0
+COT_MEM_DEVICE = 1
+
+SOLVE_REFERENCE = 0
+SOLVE_WOLFE = 1
+
+EXPORTED = [
+    "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
+    "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_last_error",
+]
+
+
+class cot_config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("bucket_size", ctypes.c_int),
+                ("warps_per_block", ctypes.c_int), ("max_ring", ctypes.c_int)]
+
+
+class cot_solve_opts(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("history", ctypes.c_int), ("max_iter", ctypes.c_int),
+                ("tol", ctypes.c_double), ("initial_step", ctypes.c_double), ("c1", ctypes.c_double),
+                ("c2", ctypes.c_double), ("max_ls", ctypes.c_int), ("use_graph", ctypes.c_int)]
+
+
+class cot_solve_stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("evaluations", ctypes.c_int), ("restarts", ctypes.c_int),
+                ("converged", ctypes.c_int), ("f", ctypes.c_double), ("max_rel_err", ctypes.c_double),
+                ("grad_norm", ctypes.c_double), ("empty_cells", ctypes.c_int),
+                ("ring_overflows", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
+class CotError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"causticot error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load the shared library (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m caustic_b200.build` (or "
+                               "__graft_entry__.build()) first; there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        up = ctypes.POINTER(ctypes.c_ubyte)
+        L.cot_version.argtypes = [ip, ip, ip]
+        L.cot_create.argtypes = [ctypes.POINTER(cot_config), ctypes.POINTER(vp)]
+        L.cot_destroy.argtypes = [vp]
+        L.cot_set_stream.argtypes = [vp, vp]
+        L.cot_set_problem.argtypes = [vp, vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+        L.cot_eval.argtypes = [vp, vp, dp, vp, vp, vp, ctypes.c_int]
+        L.cot_cells.argtypes = [vp, dp, ip, dp, ip, ctypes.c_int]
+        L.cot_solve.argtypes = [vp, vp, ctypes.POINTER(cot_solve_opts), ctypes.POINTER(cot_solve_stats), ctypes.c_int]
+        L.cot_centroids.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
+        L.cot_source_masses.argtypes = [vp, dp, ctypes.c_int, dp, dp]
+        L.cot_render.argtypes = [vp, dp, ctypes.c_double, dp]
+        L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        for name in EXPORTED:
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _vptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def version():
+    L = load()
+    a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    L.cot_version(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
+
+
+@dataclass
+class SolveStats:
+    iterations: int
+    evaluations: int
+    restarts: int
+    converged: bool
+    f: float
+    max_rel_err: float
+    grad_norm: float
+    empty_cells: int
+    ring_overflows: int
+    ms: float
+
+
+class Solver:
+    """One handle: a problem on one GPU and the calls on it.
+
+    Arrays may be numpy (host) or torch CUDA tensors (device, float64,
+    contiguous); outputs come back in the same kind as the input weights.
+    """
+
+    def __init__(self, device: int = 0, bucket_size: int = 0, warps_per_block: int = 0, max_ring: int = 0):
+        L = load()
+        self._L = L
+        cfg = cot_config(device, bucket_size, warps_per_block, max_ring)
+        h = ctypes.c_void_p()
+        rc = L.cot_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != COT_OK:
+            raise CotError(rc, self._err(None))
+        self._h = h
+        self.n = 0
+        self.device = device
+
+    def _err(self, h="self"):
+        buf = ctypes.create_string_buffer(1024)
+        self._L.cot_last_error(self._h if h == "self" else None, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc, allow=()):
+        if rc != COT_OK and rc not in allow:
+            raise CotError(rc, self._err())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cot_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._L.cot_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    # -------------------------------------------------------------------
+    def set_problem(self, xy, nu, density, size, proj_domain):
+        """size = (nx, ny): pixels along x and y, density[ix + iy*nx]."""
+        nx, ny = int(size[0]), int(size[1])
+        pd = _f64(proj_domain)
+        if _is_torch(xy):
+            self._check(self._L.cot_set_problem(self._h, _tptr(xy), _tptr(nu), int(nu.numel()), _tptr(density),
+                                                nx, ny, _dptr(pd), COT_MEM_DEVICE))
+            self.n = int(nu.numel())
+        else:
+            xy, nu, density = _f64(xy), _f64(nu), _f64(density)
+            self._keep = (xy, nu, density)
+            self._check(self._L.cot_set_problem(self._h, _vptr(xy), _vptr(nu), int(nu.size), _vptr(density),
+                                                nx, ny, _dptr(pd), COT_MEM_HOST))
+            self.n = int(nu.size)
+
+    def eval(self, w):
+        """(f, mu, g, f_cell) at weights w."""
+        f = ctypes.c_double()
+        if _is_torch(w):
+            import torch
+            mu = torch.empty_like(w)
+            g = torch.empty_like(w)
+            fc = torch.empty_like(w)
+            rc = self._L.cot_eval(self._h, _tptr(w), ctypes.byref(f), _tptr(mu), _tptr(g), _tptr(fc),
+                                  COT_MEM_DEVICE)
+        else:
+            w = _f64(w)
+            mu, g, fc = np.empty_like(w), np.empty_like(w), np.empty_like(w)
+            rc = self._L.cot_eval(self._h, _vptr(w), ctypes.byref(f), _vptr(mu), _vptr(g), _vptr(fc), COT_MEM_HOST)
+        self._check(rc)
+        return f.value, mu, g, fc
+
+    def cells(self, w):
+        """Rings of the cells inside proj_domain: (offsets[n+1], xy[V,2], nbr[V])."""
+        w = _f64(w)
+        cap = max(16 * self.n, 64)
+        while True:
+            off = np.zeros(self.n + 1, dtype=np.int32)
+            xy = np.zeros(2 * cap)
+            nb = np.zeros(cap, dtype=np.int32)
+            rc = self._L.cot_cells(self._h, _dptr(w), off.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(xy),
+                                   nb.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), cap)
+            if rc == COT_ECAPACITY:
+                cap *= 2
+                continue
+            self._check(rc)
+            V = int(off[-1])
+            return off, xy[: 2 * V].reshape(V, 2), nb[:V]
+
+    def solve(self, w0, mode=SOLVE_WOLFE, history=10, max_iter=20000, tol=1e-4, initial_step=1.0,
+              c1=0.0, c2=0.0, max_ls=0, use_graph=0, raise_on_noconv=False):
+        opts = cot_solve_opts(mode, history, max_iter, tol, initial_step, c1, c2, max_ls, use_graph)
+        st = cot_solve_stats()
+        if _is_torch(w0):
+            w = w0.clone()
+            rc = self._L.cot_solve(self._h, _tptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_DEVICE)
+        else:
+            w = _f64(w0).copy()
+            rc = self._L.cot_solve(self._h, _vptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_HOST)
+        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV,))
+        stats = SolveStats(st.iterations, st.evaluations, st.restarts, bool(st.converged), st.f, st.max_rel_err,
+                           st.grad_norm, st.empty_cells, st.ring_overflows, st.ms)
+        return w, stats
+
+    def centroids(self, w, weighted=True):
+        if _is_torch(w):
+            import torch
+            xy = torch.empty((self.n, 2), dtype=torch.float64, device=w.device)
+            ex = torch.empty(self.n, dtype=torch.uint8, device=w.device)
+            rc = self._L.cot_centroids(self._h, _tptr(w), _tptr(xy), _tptr(ex), int(bool(weighted)), COT_MEM_DEVICE)
+            self._check(rc)
+            return xy, ex.bool()
+        w = _f64(w)
+        xy = np.empty((self.n, 2))
+        ex = np.empty(self.n, dtype=np.uint8)
+        rc = self._L.cot_centroids(self._h, _vptr(w), _vptr(xy), _vptr(ex), int(bool(weighted)), COT_MEM_HOST)
+        self._check(rc)
+        return xy, ex.astype(bool)
+
+    def source_masses(self, points, sample_domain):
+        p = _f64(points).reshape(-1, 2)
+        out = np.empty(p.shape[0])
+        rc = self._L.cot_source_masses(self._h, _dptr(p), p.shape[0], _dptr(_f64(sample_domain)), _dptr(out))
+        self._check(rc)
+        return out
+
+
+def _is_torch(a):
+    return type(a).__module__.startswith("torch")
+
+
+def _tptr(t):
+    import torch
+
+    if not t.is_cuda or t.dtype not in (torch.float64, torch.uint8) or not t.is_contiguous():
+        raise ValueError("device arrays must be contiguous CUDA tensors (float64)")
+    return ctypes.c_void_p(t.data_ptr())

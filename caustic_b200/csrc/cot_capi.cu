@@ -1,0 +1,767 @@
+// C ABI of the solver (declarations and reference mapping: include/causticot.h).
+//
+// Host side of a handle: the one-time problem set-up (bucket counting sort,
+// bound-tree statistics, density scaling), the permutations between the
+// caller's site order and the bucket order used on the device, and the solve
+// loop that launches the device kernels and reads one control block per
+// line-search trial.
+#include "../../include/causticot.h"
+#include "cot_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+struct CotProblemDev {
+    int n = 0;
+    int nb = 0;
+    int nodes = 0;
+    double2 *xy = nullptr;
+    double *nu = nullptr;
+    int *bstart = nullptr;
+    int *sbucket = nullptr;
+    double4 *tstat = nullptr;
+    double4 *tdyn = nullptr;
+    double *rho = nullptr;
+    int *perm = nullptr;   // sorted -> caller index
+    std::vector<int> hperm;
+    CotGeo geo{};
+    // per evaluation
+    double *w = nullptr, *wt = nullptr, *d = nullptr, *mu = nullptr, *mut = nullptr, *fc = nullptr;
+    double *phibar = nullptr;
+    int *nv = nullptr, *ovf_list = nullptr, *ovf_count = nullptr;
+    double *partials = nullptr;
+    unsigned int *ticket = nullptr;
+    CotEvalOut *out = nullptr;
+    double *tmp = nullptr;  // caller-order staging (2n doubles)
+    // solver
+    CotSolver *S = nullptr;
+    double *Sv = nullptr, *Yv = nullptr;
+    int hist_alloc = 0;
+};
+
+struct cot_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cot_config cfg{};
+    int num_sms = 148;
+    std::string err;
+    CotProblemDev P;
+    bool has_problem = false;
+    CotSolver *hS = nullptr;  // pinned mirror of the control block
+};
+
+static std::string g_create_err;
+
+namespace cot {
+
+int fail(cot_handle *h, int code, const char *what, const char *detail)
+{
+    std::string m = std::string(what) + (detail ? std::string(": ") + detail : std::string());
+    if (h) h->err = m;
+    else g_create_err = m;
+    return code;
+}
+
+static int failf(cot_handle *h, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return fail(h, code, buf, nullptr);
+}
+
+// ---- small device helpers --------------------------------------------------
+__global__ void k_gather(int n, const int *__restrict__ perm, const double *__restrict__ src, double *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[perm[i]];
+}
+__global__ void k_scatter(int n, const int *__restrict__ perm, const double *__restrict__ src, double *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[perm[i]] = src[i];
+}
+__global__ void k_scatter2(int n, const int *__restrict__ perm, const double *__restrict__ src, double *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        dst[2 * perm[i]] = src[2 * i];
+        dst[2 * perm[i] + 1] = src[2 * i + 1];
+    }
+}
+__global__ void k_scatter_u8(int n, const int *__restrict__ perm, const unsigned char *__restrict__ src,
+                             unsigned char *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[perm[i]] = src[i];
+}
+__global__ void k_grad(int n, const double *__restrict__ mu, const double *__restrict__ nu, double *__restrict__ g)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) g[i] = mu[i] - nu[i];
+}
+
+static inline int nblk(int n) { return (n + 255) / 256; }
+
+}  // namespace cot
+
+using namespace cot;
+
+static void free_problem(CotProblemDev &P)
+{
+    void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
+                    P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_count, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
+                    P.Yv};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    P = CotProblemDev();
+}
+
+extern "C" int cot_version(int *major, int *minor, int *patch)
+{
+    if (major) *major = COT_VERSION_MAJOR;
+    if (minor) *minor = COT_VERSION_MINOR;
+    if (patch) *patch = COT_VERSION_PATCH;
+    return COT_OK;
+}
+
+extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
+{
+    if (!out) return fail(nullptr, COT_EINVAL, "cot_create: out is NULL", nullptr);
+    *out = nullptr;
+    cot_handle *h = new (std::nothrow) cot_handle();
+    if (!h) return fail(nullptr, COT_ENOMEM, "cot_create: out of host memory", nullptr);
+    if (cfg) h->cfg = *cfg;
+    if (h->cfg.bucket_size <= 0) h->cfg.bucket_size = 4;
+    if (h->cfg.warps_per_block <= 0) h->cfg.warps_per_block = 4;
+    if (h->cfg.warps_per_block > 8) h->cfg.warps_per_block = 8;
+    if (h->cfg.max_ring <= 0) h->cfg.max_ring = 200;
+    h->device = h->cfg.device;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        delete h;
+        return fail(nullptr, COT_ECUDA, "cot_create: no CUDA device", e != cudaSuccess ? cudaGetErrorString(e) : nullptr);
+    }
+    if (h->device < 0 || h->device >= ndev) {
+        delete h;
+        return fail(nullptr, COT_EINVAL, "cot_create: bad device ordinal", nullptr);
+    }
+    e = cudaSetDevice(h->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hS, sizeof(CotSolver));
+    if (e != cudaSuccess) {
+        if (h->own_stream) cudaStreamDestroy(h->own_stream);
+        delete h;
+        return fail(nullptr, COT_ECUDA, "cot_create", cudaGetErrorString(e));
+    }
+    configure_cells_kernels();
+    h->stream = h->own_stream;
+    *out = h;
+    return COT_OK;
+}
+
+extern "C" int cot_destroy(cot_handle *h)
+{
+    if (!h) return COT_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_problem(h->P);
+    if (h->hS) cudaFreeHost(h->hS);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return COT_OK;
+}
+
+extern "C" int cot_set_stream(cot_handle *h, void *s)
+{
+    if (!h) return COT_EINVAL;
+    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return COT_OK;
+}
+
+extern "C" int cot_last_error(cot_handle *h, char *buf, size_t n)
+{
+    const std::string &m = h ? h->err : g_create_err;
+    if (!buf || n == 0) return COT_EINVAL;
+    std::snprintf(buf, n, "%s", m.c_str());
+    return COT_OK;
+}
+
+// Read caller data (host or device) into a host vector.
+static int to_host(cot_handle *h, const double *src, size_t count, int mem, std::vector<double> &dst)
+{
+    dst.resize(count);
+    if (count == 0) return COT_OK;
+    if (mem == COT_MEM_DEVICE) {
+        COT_CUDA_TRY(cudaMemcpyAsync(dst.data(), src, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    } else {
+        std::memcpy(dst.data(), src, count * sizeof(double));
+    }
+    return COT_OK;
+}
+
+// Build the device problem: bucket grid over the sites, counting sort
+// (bucket, then caller index), bound-tree statistics, density scaled to
+// sum(nu) per unit area.
+static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<double> &xy,
+                         const std::vector<double> &nu, const std::vector<double> &dens, int nx, int ny,
+                         const double pd[4])
+{
+    const int n = (int)nu.size();
+    cudaStream_t s = h->stream;
+    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    for (int i = 0; i < n; i++) {
+        double x = xy[2 * i], y = xy[2 * i + 1];
+        if (!std::isfinite(x) || !std::isfinite(y)) return failf(h, COT_EINVAL, "site %d is not finite", i);
+        xmin = std::min(xmin, x); xmax = std::max(xmax, x);
+        ymin = std::min(ymin, y); ymax = std::max(ymax, y);
+    }
+    double L = std::max({pd[1] - pd[0], pd[3] - pd[2], xmax - xmin, ymax - ymin,
+                         std::fabs(pd[0]), std::fabs(pd[1]), std::fabs(pd[2]), std::fabs(pd[3])});
+    if (!(L > 0)) L = 1.0;
+    double wx = std::max(xmax - xmin, 1e-9 * L), wy = std::max(ymax - ymin, 1e-9 * L);
+    wx *= 1.0 + 1e-12;
+    wy *= 1.0 + 1e-12;
+    int bs = h->cfg.bucket_size;
+    double nbt = std::max(1.0, (double)n / bs);
+    int bx = std::max(1, (int)std::llround(std::sqrt(nbt * wx / wy)));
+    int by = std::max(1, (int)std::llround(nbt / bx));
+    bx = std::min(bx, 1 << 15);
+    by = std::min(by, 1 << 15);
+    const int nb = bx * by;
+    double hx = wx / bx, hy = wy / by;
+    double ihx = 1.0 / hx, ihy = 1.0 / hy;
+    std::vector<int> bucket(n), cnt(nb + 1, 0);
+    for (int i = 0; i < n; i++) {
+        int u = (int)((xy[2 * i] - xmin) * ihx), v = (int)((xy[2 * i + 1] - ymin) * ihy);
+        u = std::min(std::max(u, 0), bx - 1);
+        v = std::min(std::max(v, 0), by - 1);
+        bucket[i] = u + v * bx;
+        cnt[bucket[i] + 1]++;
+    }
+    for (int b = 0; b < nb; b++) cnt[b + 1] += cnt[b];
+    std::vector<int> cur(cnt.begin(), cnt.end() - 1), perm(n), sb(n);
+    for (int i = 0; i < n; i++) {
+        int p = cur[bucket[i]]++;
+        perm[p] = i;
+        sb[p] = bucket[i];
+    }
+    std::vector<double> sxy(2 * (size_t)n), snu(n);
+    for (int p = 0; p < n; p++) {
+        sxy[2 * p] = xy[2 * perm[p]];
+        sxy[2 * p + 1] = xy[2 * perm[p] + 1];
+        snu[p] = nu[perm[p]];
+    }
+    // tree statistics
+    std::vector<int> off, lw, lh;
+    int W = bx, H = by, total = 0;
+    while (true) {
+        off.push_back(total);
+        lw.push_back(W);
+        lh.push_back(H);
+        total += W * H;
+        if (W == 1 && H == 1) break;
+        W = (W + 1) / 2;
+        H = (H + 1) / 2;
+        if ((int)off.size() >= COT_MAX_LEVELS) return failf(h, COT_EINVAL, "too many tree levels");
+    }
+    const int nlev = (int)off.size();
+    std::vector<double4> tst(total);
+    for (int b = 0; b < nb; b++) {
+        int s0 = cnt[b], s1 = cnt[b + 1];
+        double mx = 0, my = 0;
+        for (int p = s0; p < s1; p++) { mx += sxy[2 * p]; my += sxy[2 * p + 1]; }
+        int c = s1 - s0;
+        if (c > 0) { mx /= c; my /= c; }
+        double r = 0;
+        for (int p = s0; p < s1; p++) r = std::max(r, std::hypot(sxy[2 * p] - mx, sxy[2 * p + 1] - my));
+        r = r * (1.0 + 1e-12) + 1e-15 * L;
+        tst[b] = make_double4(mx, my, r, (double)c);
+    }
+    for (int l = 1; l < nlev; l++) {
+        for (int v = 0; v < lh[l]; v++)
+            for (int u = 0; u < lw[l]; u++) {
+                double c = 0, mx = 0, my = 0;
+                for (int bb = 0; bb < 2; bb++)
+                    for (int aa = 0; aa < 2; aa++) {
+                        int uu = 2 * u + aa, vv = 2 * v + bb;
+                        if (uu >= lw[l - 1] || vv >= lh[l - 1]) continue;
+                        double4 ch = tst[off[l - 1] + uu + vv * lw[l - 1]];
+                        c += ch.w; mx += ch.w * ch.x; my += ch.w * ch.y;
+                    }
+                if (c > 0) { mx /= c; my /= c; }
+                double r = 0;
+                for (int bb = 0; bb < 2; bb++)
+                    for (int aa = 0; aa < 2; aa++) {
+                        int uu = 2 * u + aa, vv = 2 * v + bb;
+                        if (uu >= lw[l - 1] || vv >= lh[l - 1]) continue;
+                        double4 ch = tst[off[l - 1] + uu + vv * lw[l - 1]];
+                        if (ch.w <= 0) continue;
+                        r = std::max(r, std::hypot(ch.x - mx, ch.y - my) + ch.z);
+                    }
+                r = r * (1.0 + 1e-12) + 1e-15 * L;
+                tst[off[l] + u + v * lw[l]] = make_double4(mx, my, r, c);
+            }
+    }
+    // density per unit area, summing to sum(nu) over the domain
+    double area_scalar = 0, dsum = 0;
+    for (int i = 0; i < n; i++) area_scalar += nu[i];
+    for (size_t p = 0; p < dens.size(); p++) {
+        if (!std::isfinite(dens[p]) || dens[p] < 0) return failf(h, COT_EINVAL, "density pixel %zu is negative or not finite", p);
+        dsum += dens[p];
+    }
+    if (!(dsum > 0)) return failf(h, COT_EINVAL, "density sums to zero");
+    const double xs = (pd[1] - pd[0]) / (double)nx, ys = (pd[3] - pd[2]) / (double)ny;
+    const double ga = xs * ys;
+    const double gray = dsum / area_scalar;
+    std::vector<double> rho(dens.size());
+    for (size_t p = 0; p < dens.size(); p++) rho[p] = (dens[p] / gray) / ga;
+
+    free_problem(P);
+    P.n = n;
+    P.nb = nb;
+    P.nodes = total;
+    P.hperm = perm;
+    size_t N = (size_t)n;
+    auto A = [&](void **p, size_t bytes) -> cudaError_t { return cudaMalloc(p, bytes > 0 ? bytes : 16); };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = A((void **)&P.xy, N * sizeof(double2));
+    if (e == cudaSuccess) e = A((void **)&P.nu, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.bstart, (nb + 1) * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.sbucket, N * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.tstat, total * sizeof(double4));
+    if (e == cudaSuccess) e = A((void **)&P.tdyn, total * sizeof(double4));
+    if (e == cudaSuccess) e = A((void **)&P.rho, rho.size() * 8);
+    if (e == cudaSuccess) e = A((void **)&P.perm, N * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.w, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.wt, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.d, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.mu, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.mut, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.fc, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
+    if (e == cudaSuccess) e = A((void **)&P.nv, N * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.ovf_list, N * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.ovf_count, sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.partials, (size_t)reduce_blocks(n) * (5 * COT_MAX_HIST + 8) * 8);
+    if (e == cudaSuccess) e = A((void **)&P.ticket, sizeof(unsigned int));
+    if (e == cudaSuccess) e = A((void **)&P.out, sizeof(CotEvalOut));
+    if (e == cudaSuccess) e = A((void **)&P.tmp, 2 * N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.S, sizeof(CotSolver));
+    if (e != cudaSuccess) {
+        free_problem(P);
+        return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
+    }
+    COT_CUDA_TRY(cudaMemcpyAsync(P.xy, sxy.data(), N * sizeof(double2), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.nu, snu.data(), N * 8, cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.bstart, cnt.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.sbucket, sb.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.tstat, tst.data(), total * sizeof(double4), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, sizeof(int), s));
+    COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
+
+    CotGeo &g = P.geo;
+    g = CotGeo{};
+    g.n = n;
+    g.xy = P.xy;
+    g.nu = P.nu;
+    g.bstart = P.bstart;
+    g.sbucket = P.sbucket;
+    g.bx = bx;
+    g.by = by;
+    g.ox = xmin;
+    g.oy = ymin;
+    g.ihx = ihx;
+    g.ihy = ihy;
+    g.nlev = nlev;
+    for (int l = 0; l < nlev; l++) {
+        g.lev_off[l] = off[l];
+        g.lev_w[l] = lw[l];
+        g.lev_h[l] = lh[l];
+    }
+    g.tstat = P.tstat;
+    g.tdyn = P.tdyn;
+    g.rho = P.rho;
+    g.nx = nx;
+    g.ny = ny;
+    for (int k = 0; k < 4; k++) g.pd[k] = pd[k];
+    g.xs = xs;
+    g.ys = ys;
+    g.margin = 1e-11 * L * L;
+    return COT_OK;
+}
+
+extern "C" int cot_set_problem(cot_handle *h, const double *sites_xy, const double *nu, int n,
+                               const double *density, int nx, int ny, const double proj_domain[4], int mem)
+{
+    if (!h) return COT_EINVAL;
+    if (n <= 0 || !sites_xy || !nu || !density || nx <= 0 || ny <= 0 || !proj_domain)
+        return fail(h, COT_EINVAL, "cot_set_problem: bad argument", nullptr);
+    if (mem != COT_MEM_HOST && mem != COT_MEM_DEVICE) return fail(h, COT_EINVAL, "cot_set_problem: bad mem flag", nullptr);
+    const double *pd = proj_domain;
+    if (!(pd[1] > pd[0]) || !(pd[3] > pd[2]) || !std::isfinite(pd[0]) || !std::isfinite(pd[1]) ||
+        !std::isfinite(pd[2]) || !std::isfinite(pd[3]))
+        return fail(h, COT_EINVAL, "cot_set_problem: empty or non-finite proj_domain", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    std::vector<double> xy, vnu, dens;
+    int r;
+    if ((r = to_host(h, sites_xy, 2 * (size_t)n, mem, xy)) != COT_OK) return r;
+    if ((r = to_host(h, nu, (size_t)n, mem, vnu)) != COT_OK) return r;
+    if ((r = to_host(h, density, (size_t)nx * ny, mem, dens)) != COT_OK) return r;
+    for (int i = 0; i < n; i++)
+        if (!(vnu[i] > 0) || !std::isfinite(vnu[i])) return failf(h, COT_EINVAL, "cot_set_problem: nu[%d] must be positive", i);
+    h->has_problem = false;
+    r = build_problem(h, h->P, xy, vnu, dens, nx, ny, pd);
+    if (r != COT_OK) return r;
+    h->has_problem = true;
+    return COT_OK;
+}
+
+// Caller-order vector -> sorted device vector.
+static int upload_sorted(cot_handle *h, const double *src, int mem, double *dst)
+{
+    CotProblemDev &P = h->P;
+    size_t N = (size_t)P.n;
+    if (mem == COT_MEM_DEVICE) {
+        k_gather<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, src, dst);
+    } else {
+        COT_CUDA_TRY(cudaMemcpyAsync(P.tmp, src, N * 8, cudaMemcpyHostToDevice, h->stream));
+        k_gather<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, P.tmp, dst);
+    }
+    COT_CUDA_TRY(cudaGetLastError());
+    return COT_OK;
+}
+
+// Sorted device vector -> caller-order vector.
+static int download_sorted(cot_handle *h, const double *src, double *dst, int mem)
+{
+    CotProblemDev &P = h->P;
+    size_t N = (size_t)P.n;
+    if (mem == COT_MEM_DEVICE) {
+        k_scatter<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, src, dst);
+    } else {
+        k_scatter<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, src, P.tmp);
+        COT_CUDA_TRY(cudaMemcpyAsync(dst, P.tmp, N * 8, cudaMemcpyDeviceToHost, h->stream));
+    }
+    COT_CUDA_TRY(cudaGetLastError());
+    return COT_OK;
+}
+
+static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, const double *tptr)
+{
+    CellsArgs a{};
+    a.w = w;
+    a.d = d;
+    a.tptr = tptr;
+    a.wt = P.wt;
+    a.phibar = P.phibar;
+    a.mu = P.mut;
+    a.fc = P.fc;
+    a.nv = P.nv;
+    a.ovf_list = P.ovf_list;
+    a.ovf_count = P.ovf_count;
+    return a;
+}
+
+extern "C" int cot_eval(cot_handle *h, const double *w, double *f_total, double *mu, double *g, double *f_cell,
+                        int mem)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_eval: no problem set", nullptr);
+    if (!w) return fail(h, COT_EINVAL, "cot_eval: w is NULL", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    int r;
+    if ((r = upload_sorted(h, w, mem, P.w)) != COT_OK) return r;
+    CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, s);
+    COT_CUDA_TRY(cudaGetLastError());
+    CotEvalOut o;
+    COT_CUDA_TRY(cudaMemcpyAsync(&o, P.out, sizeof o, cudaMemcpyDeviceToHost, s));
+    if (mu && (r = download_sorted(h, P.mut, mu, mem)) != COT_OK) return r;
+    if (f_cell && (r = download_sorted(h, P.fc, f_cell, mem)) != COT_OK) return r;
+    if (g) {
+        k_grad<<<nblk(P.n), 256, 0, s>>>(P.n, P.mut, P.nu, P.d);
+        if ((r = download_sorted(h, P.d, g, mem)) != COT_OK) return r;
+    }
+    COT_CUDA_TRY(cudaStreamSynchronize(s));
+    if (f_total) *f_total = o.f;
+    if (o.maxnv > 256) return failf(h, COT_ERING, "cot_eval: a cell has more than 256 vertices");
+    return COT_OK;
+}
+
+extern "C" int cot_cells(cot_handle *h, const double *w, int *ring_offsets, double *ring_xy, int *ring_nbr,
+                         int capacity)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_cells: no problem set", nullptr);
+    if (!w || !ring_offsets) return fail(h, COT_EINVAL, "cot_cells: NULL argument", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    const int cap = 256;
+    size_t N = (size_t)P.n;
+    double *rxy = nullptr;
+    int *rlab = nullptr;
+    COT_CUDA_TRY(cudaMalloc(&rxy, N * cap * 2 * 8));
+    cudaError_t e = cudaMalloc(&rlab, N * cap * sizeof(int));
+    if (e != cudaSuccess) {
+        cudaFree(rxy);
+        return fail(h, COT_ENOMEM, "cot_cells: device allocation", cudaGetErrorString(e));
+    }
+    int r = upload_sorted(h, w, COT_MEM_HOST, P.w);
+    std::vector<double> hxy;
+    std::vector<int> hlab, hnv(N);
+    if (r == COT_OK) {
+        CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+        a.ring_xy = rxy;
+        a.ring_lab = rlab;
+        a.ring_cap = cap;
+        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+        hxy.resize(N * cap * 2);
+        hlab.resize(N * cap);
+        e = cudaMemcpyAsync(hxy.data(), rxy, N * cap * 2 * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hlab.data(), rlab, N * cap * sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hnv.data(), P.nv, N * sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) r = fail(h, COT_ECUDA, "cot_cells", cudaGetErrorString(e));
+    }
+    cudaFree(rxy);
+    cudaFree(rlab);
+    if (r != COT_OK) return r;
+    // caller order, CSR
+    std::vector<int> byc(N);
+    for (size_t p = 0; p < N; p++) byc[P.hperm[p]] = (int)p;
+    int o = 0;
+    for (size_t i = 0; i < N; i++) {
+        int p = byc[i];
+        int m = hnv[p];
+        if (m > cap) return failf(h, COT_ERING, "cot_cells: cell %zu has more than %d vertices", i, cap);
+        ring_offsets[i] = o;
+        if (o + m > capacity) return failf(h, COT_ECAPACITY, "cot_cells: capacity %d too small", capacity);
+        for (int k = 0; k < m; k++) {
+            if (ring_xy) {
+                ring_xy[2 * (o + k)] = hxy[2 * ((size_t)p * cap + k)];
+                ring_xy[2 * (o + k) + 1] = hxy[2 * ((size_t)p * cap + k) + 1];
+            }
+            if (ring_nbr) {
+                int l = hlab[(size_t)p * cap + k];
+                ring_nbr[o + k] = l >= 0 ? P.hperm[l] : l;
+            }
+        }
+        o += m;
+    }
+    ring_offsets[N] = o;
+    return COT_OK;
+}
+
+extern "C" int cot_centroids(cot_handle *h, const double *w, double *xy, unsigned char *exist, int weighted, int mem)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_centroids: no problem set", nullptr);
+    if (!w || !xy || !exist) return fail(h, COT_EINVAL, "cot_centroids: NULL argument", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    size_t N = (size_t)P.n;
+    int r;
+    if ((r = upload_sorted(h, w, mem, P.w)) != COT_OK) return r;
+    double *cen = nullptr;
+    unsigned char *ex = nullptr, *ex2 = nullptr;
+    COT_CUDA_TRY(cudaMalloc(&cen, N * 2 * 8 * 2));
+    cudaError_t e = cudaMalloc(&ex, N * 2);
+    if (e != cudaSuccess) {
+        cudaFree(cen);
+        return fail(h, COT_ENOMEM, "cot_centroids: device allocation", cudaGetErrorString(e));
+    }
+    ex2 = ex + N;
+    CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+    a.cen = cen;
+    a.exist = ex;
+    a.weighted = weighted ? 1 : 0;
+    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+    double *cen2 = cen + 2 * N;
+    k_scatter2<<<nblk(P.n), 256, 0, s>>>(P.n, P.perm, cen, cen2);
+    k_scatter_u8<<<nblk(P.n), 256, 0, s>>>(P.n, P.perm, ex, ex2);
+    cudaMemcpyKind k = mem == COT_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    e = cudaMemcpyAsync(xy, cen2, N * 2 * 8, k, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(exist, ex2, N, k, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(cen);
+    cudaFree(ex);
+    if (e != cudaSuccess) return fail(h, COT_ECUDA, "cot_centroids", cudaGetErrorString(e));
+    return COT_OK;
+}
+
+extern "C" int cot_source_masses(cot_handle *h, const double *points_xy, int n, const double sample_domain[4],
+                                 double *nu_out)
+{
+    if (!h) return COT_EINVAL;
+    if (!points_xy || n <= 0 || !sample_domain || !nu_out) return fail(h, COT_EINVAL, "cot_source_masses: bad argument", nullptr);
+    const double *sd = sample_domain;
+    if (!(sd[1] > sd[0]) || !(sd[3] > sd[2])) return fail(h, COT_EINVAL, "cot_source_masses: empty sample_domain", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    // unweighted cells inside the sample domain, one "pixel" of unit density
+    std::vector<double> xy(points_xy, points_xy + 2 * (size_t)n), one(n, 1.0), dens(1, 1.0);
+    CotProblemDev Q;
+    int r = build_problem(h, Q, xy, one, dens, 1, 1, sd);
+    if (r != COT_OK) return r;
+    cudaStream_t s = h->stream;
+    std::vector<double> area(n), sorted(n);
+    cudaError_t e = cudaMemsetAsync(Q.w, 0, (size_t)n * 8, s);
+    if (e == cudaSuccess) {
+        CellsArgs a = cells_args(Q, Q.w, nullptr, nullptr);
+        launch_eval(Q.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+        e = cudaMemcpyAsync(sorted.data(), Q.mut, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    std::vector<int> perm = Q.hperm;
+    free_problem(Q);
+    if (e != cudaSuccess) return fail(h, COT_ECUDA, "cot_source_masses", cudaGetErrorString(e));
+    // the density above integrates to n over the domain: rho = n / area; undo
+    const double dom = (sd[1] - sd[0]) * (sd[3] - sd[2]);
+    double tot = 0;
+    for (int p = 0; p < n; p++) {
+        area[perm[p]] = sorted[p] * dom / (double)n;
+    }
+    for (int i = 0; i < n; i++) tot += area[i];
+    if (!(tot > 0)) return fail(h, COT_EINVAL, "cot_source_masses: zero total area", nullptr);
+    for (int i = 0; i < n; i++) nu_out[i] = area[i] / tot * dom;
+    return COT_OK;
+}
+
+extern "C" int cot_render(cot_handle *h, const double *w, double gray_multiple, double *out)
+{
+    (void)w;
+    (void)gray_multiple;
+    (void)out;
+    if (!h) return COT_EINVAL;
+    return fail(h, COT_EINVAL, "cot_render: not available in this build", nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// solve
+// ---------------------------------------------------------------------------
+extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts, cot_solve_stats *stats, int mem)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_solve: no problem set", nullptr);
+    if (!w_inout || !opts) return fail(h, COT_EINVAL, "cot_solve: NULL argument", nullptr);
+    cot_solve_opts o = *opts;
+    if (o.mode != COT_SOLVE_REFERENCE && o.mode != COT_SOLVE_WOLFE) return fail(h, COT_EINVAL, "cot_solve: bad mode", nullptr);
+    if (o.history <= 0 || o.history > COT_MAX_HIST) return failf(h, COT_EINVAL, "cot_solve: history must be in 1..%d", COT_MAX_HIST);
+    if (o.max_iter < 0) return fail(h, COT_EINVAL, "cot_solve: max_iter < 0", nullptr);
+    if (!(o.initial_step > 0)) o.initial_step = 1.0;
+    if (!(o.c1 > 0)) o.c1 = 1e-4;
+    if (!(o.c2 > 0)) o.c2 = 0.9;
+    if (o.max_ls <= 0) o.max_ls = 30;
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    const int n = P.n;
+    const int m = o.history;
+    if (P.hist_alloc < m) {
+        if (P.Sv) cudaFree(P.Sv);
+        if (P.Yv) cudaFree(P.Yv);
+        P.Sv = P.Yv = nullptr;
+        P.hist_alloc = 0;
+        cudaError_t e = cudaMalloc(&P.Sv, (size_t)m * n * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&P.Yv, (size_t)m * n * 8);
+        if (e != cudaSuccess) return fail(h, COT_ENOMEM, "cot_solve: history allocation", cudaGetErrorString(e));
+        P.hist_alloc = m;
+    }
+    COT_CUDA_TRY(cudaMemsetAsync(P.Sv, 0, (size_t)m * n * 8, s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.Yv, 0, (size_t)m * n * 8, s));
+    CotSolver &hs = *h->hS;
+    std::memset(&hs, 0, sizeof hs);
+    hs.mode = o.mode;
+    hs.m = m;
+    hs.max_ls = o.max_ls;
+    hs.max_iter = o.max_iter;
+    hs.max_ring = h->cfg.max_ring;
+    hs.c1 = o.c1;
+    hs.c2 = o.c2;
+    hs.t0 = o.initial_step;
+    hs.tol = o.tol;
+    hs.H0 = 1.0;
+    hs.f = INFINITY;
+    if (o.max_iter == 0) hs.done = 1;
+    COT_CUDA_TRY(cudaMemcpyAsync(P.S, &hs, sizeof(CotSolver), cudaMemcpyHostToDevice, s));
+    int r;
+    if ((r = upload_sorted(h, w_inout, mem, P.w)) != COT_OK) return r;
+    cudaEvent_t e0, e1;
+    COT_CUDA_TRY(cudaEventCreate(&e0));
+    COT_CUDA_TRY(cudaEventCreate(&e1));
+    COT_CUDA_TRY(cudaEventRecord(e0, s));
+    // first point
+    {
+        CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+        launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, s);
+        launch_init_from_eval(P.S, P.out, s);
+        launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, s);
+    }
+    const size_t ctl = 16 * sizeof(int);
+    int guard = 0;
+    while (true) {
+        launch_begin_iteration(P.S, s);
+        launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, s);
+        COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
+        COT_CUDA_TRY(cudaStreamSynchronize(s));
+        if (hs.done) break;
+        double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
+        while (true) {
+            CellsArgs a = cells_args(P, P.w, P.d, tptr);
+            launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+            launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, s);
+            COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
+            COT_CUDA_TRY(cudaStreamSynchronize(s));
+            if (!hs.ls_active) break;
+            if (++guard > 100000000) break;
+        }
+        if (hs.accepted)
+            launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, s);
+        else
+            launch_reject(P.S, s);
+        COT_CUDA_TRY(cudaGetLastError());
+    }
+    COT_CUDA_TRY(cudaEventRecord(e1, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
+    if ((r = download_sorted(h, P.w, w_inout, mem)) != COT_OK) return r;
+    COT_CUDA_TRY(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        stats->iterations = hs.iter;
+        stats->evaluations = hs.evals;
+        stats->restarts = hs.restarts;
+        stats->converged = hs.converged;
+        stats->f = hs.f;
+        stats->max_rel_err = hs.maxrel;
+        stats->grad_norm = std::sqrt(hs.gnorm2);
+        stats->empty_cells = hs.empty;
+        stats->ring_overflows = hs.ring_rejects;
+        stats->ms = ms;
+    }
+    if (!hs.converged) return failf(h, COT_ENOTCONV, "cot_solve: stopped after %d iterations (max rel err %.3e)", hs.iter, hs.maxrel);
+    return COT_OK;
+}

@@ -1,0 +1,820 @@
+// Power cells and their pixel integrals, one warp per cell.
+//
+// Replaces, per objective evaluation, the CPU power diagram of the reference
+// (polygons_in_VD, power_diagram.cpp:8-134) and its per-cell CUDA kernels
+// compute_inte / compute_f / compute_center (basic_function.cuh:743-1191).
+//
+// Cell i is built as   proj_domain ∩ { x : |x-s_i|^2 - w_i <= |x-s_j|^2 - w_j }
+// over the sites j that can reach it.  Working relative to s_i (x = s_i + x')
+// the half-plane of neighbour j is   e.x' <= (|e|^2 - (w_j - w_i)) / 2,
+// e = s_j - s_i.  Candidates come from the 3x3 neighbour buckets around s_i;
+// completeness is certified with plane bounds: writing phi_j = (|s_j|^2-w_j)/2
+// and P_j(x) = x.s_j - phi_j (cell i = where P_i is the largest), every tree
+// node holds {c, A, m, r} with  P_j(x) <= A + (x-c).m + |x-c| r  for all its
+// sites.  c is anchored where the node's cells lie (the local slope of phi),
+// so the bound stays tight when cells sit far from their sites.  A node whose
+// bound is below P_i at every vertex of the current polygon cannot cut the
+// cell (a convex bound minus a linear function peaks at a vertex).
+//
+// The integration clips nothing: for each pixel of the cell's bounding box the
+// exact integrals of 1, x, y and |x-s_i|^2 over cell ∩ pixel are boundary sums
+// (Green's theorem in the x-dy form): the polygon edges clipped to the pixel,
+// plus the pixel's two vertical sides where they lie inside the cell.  Fully
+// covered pixels take a closed form.
+#include "cot_common.cuh"
+#include <math.h>
+
+namespace cot {
+
+#define FULLMASK 0xffffffffu
+#define COT_FRMAX 96
+#define COT_WIN 1  // window radius in buckets
+
+// ---------------------------------------------------------------------------
+// bucket and tree plane bounds (per evaluation)
+// ---------------------------------------------------------------------------
+
+// wt = w + t*d (t read from the device), phibar[b] = mean_j phi_j.
+__global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const double *__restrict__ d,
+                             const double *__restrict__ tptr, double *__restrict__ wt,
+                             double *__restrict__ phibar)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    int nb = g.bx * g.by;
+    if (b >= nb) return;
+    double t = (d != nullptr && tptr != nullptr) ? *tptr : 0.0;
+    int s0 = g.bstart[b], s1 = g.bstart[b + 1];
+    double acc = 0.0;
+    for (int j = s0; j < s1; j++) {
+        double wj = w[j];
+        // no contraction: the trial point is w + t*d exactly as written
+        if (d != nullptr) wj = __dadd_rn(wj, __dmul_rn(t, d[j]));
+        wt[j] = wj;
+        double2 s = g.xy[j];
+        acc += 0.5 * (s.x * s.x + s.y * s.y - wj);
+    }
+    phibar[b] = (s1 > s0) ? acc / (double)(s1 - s0) : 0.0;
+}
+
+// c_b = slope of phi across the neighbouring buckets, A_b = max_j c_b.s_j - phi_j.
+__global__ void k_bucket_bound(CotGeo g, const double *__restrict__ wt, const double *__restrict__ phibar)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    int nb = g.bx * g.by;
+    if (b >= nb) return;
+    double4 st = g.tstat[b];
+    if (st.w <= 0.0) {
+        g.tdyn[b] = make_double4(0.0, 0.0, -INFINITY, 0.0);
+        return;
+    }
+    int u = b % g.bx, v = b / g.bx;
+    double pb = phibar[b];
+    double c[2];
+    for (int ax = 0; ax < 2; ax++) {
+        int bp = -1, bm = -1;
+        if (ax == 0) {
+            if (u + 1 < g.bx && g.tstat[b + 1].w > 0.0) bp = b + 1;
+            if (u > 0 && g.tstat[b - 1].w > 0.0) bm = b - 1;
+        } else {
+            if (v + 1 < g.by && g.tstat[b + g.bx].w > 0.0) bp = b + g.bx;
+            if (v > 0 && g.tstat[b - g.bx].w > 0.0) bm = b - g.bx;
+        }
+        double mb = ax == 0 ? st.x : st.y;
+        double val;
+        if (bp >= 0 && bm >= 0) {
+            double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
+            double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
+            val = (phibar[bp] - phibar[bm]) / (mp - mm);
+        } else if (bp >= 0) {
+            double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
+            val = (phibar[bp] - pb) / (mp - mb);
+        } else if (bm >= 0) {
+            double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
+            val = (pb - phibar[bm]) / (mb - mm);
+        } else {
+            val = mb;
+        }
+        if (!isfinite(val)) val = mb;
+        c[ax] = val;
+    }
+    double A = -INFINITY;
+    int s0 = g.bstart[b], s1 = g.bstart[b + 1];
+    for (int j = s0; j < s1; j++) {
+        double2 s = g.xy[j];
+        double phi = 0.5 * (s.x * s.x + s.y * s.y - wt[j]);
+        A = fmax(A, c[0] * s.x + c[1] * s.y - phi);
+    }
+    g.tdyn[b] = make_double4(c[0], c[1], A, 0.0);
+}
+
+// Level L node = union of up to 2x2 level L-1 nodes.
+__global__ void k_tree_level(CotGeo g, int L)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    int W = g.lev_w[L], H = g.lev_h[L];
+    if (q >= W * H) return;
+    int node = g.lev_off[L] + q;
+    double4 st = g.tstat[node];
+    if (st.w <= 0.0) {
+        g.tdyn[node] = make_double4(0.0, 0.0, -INFINITY, 0.0);
+        return;
+    }
+    int u = q % W, v = q / W;
+    int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1], co = g.lev_off[L - 1];
+    double cx = 0.0, cy = 0.0;
+    int cnt = 0;
+    for (int bb = 0; bb < 2; bb++)
+        for (int aa = 0; aa < 2; aa++) {
+            int uu = 2 * u + aa, vv = 2 * v + bb;
+            if (uu >= cw || vv >= ch) continue;
+            int cn = co + uu + vv * cw;
+            if (g.tstat[cn].w <= 0.0) continue;
+            double4 dy = g.tdyn[cn];
+            cx += dy.x;
+            cy += dy.y;
+            cnt++;
+        }
+    cx /= cnt;
+    cy /= cnt;
+    double A = -INFINITY;
+    for (int bb = 0; bb < 2; bb++)
+        for (int aa = 0; aa < 2; aa++) {
+            int uu = 2 * u + aa, vv = 2 * v + bb;
+            if (uu >= cw || vv >= ch) continue;
+            int cn = co + uu + vv * cw;
+            double4 cs = g.tstat[cn];
+            if (cs.w <= 0.0) continue;
+            double4 dy = g.tdyn[cn];
+            double dx = cx - dy.x, dyy = cy - dy.y;
+            A = fmax(A, dy.z + dx * cs.x + dyy * cs.y + sqrt(dx * dx + dyy * dyy) * cs.z);
+        }
+    g.tdyn[node] = make_double4(cx, cy, A, 0.0);
+}
+
+// ---------------------------------------------------------------------------
+// warp helpers
+// ---------------------------------------------------------------------------
+
+// Side of a point w.r.t. a * x + b * y <= c (> 0 means outside).  One explicit
+// fused form so that every lane evaluating the same vertex gets the same bits.
+__device__ __forceinline__ double side(double a, double b, double c, double x, double y)
+{
+    return __fma_rn(a, x, __fma_rn(b, y, -c));
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FULLMASK, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(FULLMASK, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULLMASK, v, o));
+    return v;
+}
+
+// Intersection of lines a1 x + b1 y = c1 and a2 x + b2 y = c2.  Axis-aligned
+// lines are solved directly so that vertices on the domain sides sit exactly on
+// them.  Returns false for (near) parallel lines.
+__device__ __forceinline__ bool line_meet(double a1, double b1, double c1, double a2, double b2,
+                                          double c2, double &x, double &y)
+{
+    if (b1 == 0.0 && a1 != 0.0) {
+        x = c1 / a1;
+        if (b2 == 0.0) return false;
+        y = (c2 - a2 * x) / b2;
+        return true;
+    }
+    if (a1 == 0.0 && b1 != 0.0) {
+        y = c1 / b1;
+        if (a2 == 0.0) return false;
+        x = (c2 - b2 * y) / a2;
+        return true;
+    }
+    if (b2 == 0.0 && a2 != 0.0) {
+        x = c2 / a2;
+        y = (c1 - a1 * x) / b1;
+        return true;
+    }
+    if (a2 == 0.0 && b2 != 0.0) {
+        y = c2 / b2;
+        x = (c1 - b1 * y) / a1;
+        return true;
+    }
+    double det = a1 * b2 - a2 * b1;
+    double sc = (fabs(a1) + fabs(b1)) * (fabs(a2) + fabs(b2));
+    if (!(fabs(det) > 1e-13 * sc)) return false;
+    x = (c1 * b2 - c2 * b1) / det;
+    y = (a1 * c2 - a2 * c1) / det;
+    return true;
+}
+
+template <int MAXV>
+struct WarpPoly {
+    double X[MAXV], Y[MAXV];          // vertices, relative to the site
+    double A[MAXV], B[MAXV], C[MAXV]; // line of the edge leaving each vertex
+    int L[MAXV];                      // its generator (site, or -1..-4)
+    int fr[2][COT_FRMAX];             // tree traversal lists
+    double elo[33], ehi[33];          // section of the cell at column lines
+    double slo[32], shi[32];          // y-range of the cell in each column strip
+    unsigned char lv[33], rv[33];     // left / right limit of the section valid
+};
+
+// Clip the polygon by a x + b y <= c (generator lab).  Returns the new vertex
+// count, or -1 when it would exceed MAXV.
+template <int MAXV>
+__device__ int clip_poly(WarpPoly<MAXV> &P, int nv, double a, double b, double c, int lab, int lane)
+{
+    constexpr int SPL = MAXV / 32;
+    double x[SPL], y[SPL], la[SPL], lb[SPL], lc[SPL], ix[SPL], iy[SPL];
+    int ll[SPL], cnt[SPL], pos[SPL];
+    bool in[SPL], inn[SPL];
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+        int k = lane + 32 * q;
+        cnt[q] = 0;
+        in[q] = inn[q] = false;
+        if (k < nv) {
+            int kn = (k + 1 == nv) ? 0 : k + 1;
+            x[q] = P.X[k];
+            y[q] = P.Y[k];
+            double xn = P.X[kn], yn = P.Y[kn];
+            double d0 = side(a, b, c, x[q], y[q]);
+            double d1 = side(a, b, c, xn, yn);
+            in[q] = d0 <= 0.0;
+            inn[q] = d1 <= 0.0;
+            la[q] = P.A[k];
+            lb[q] = P.B[k];
+            lc[q] = P.C[k];
+            ll[q] = P.L[k];
+            cnt[q] = (in[q] ? 1 : 0) + ((in[q] != inn[q]) ? 1 : 0);
+            if (in[q] != inn[q]) {
+                if (!line_meet(la[q], lb[q], lc[q], a, b, c, ix[q], iy[q])) {
+                    double t = d0 / (d0 - d1);
+                    ix[q] = x[q] + t * (xn - x[q]);
+                    iy[q] = y[q] + t * (yn - y[q]);
+                }
+            }
+        }
+    }
+    int base = 0;
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+        int inc = warp_incl_scan(cnt[q], lane);
+        pos[q] = base + inc - cnt[q];
+        base += __shfl_sync(FULLMASK, inc, 31);
+    }
+    if (base > MAXV) return -1;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < SPL; q++) {
+        int k = lane + 32 * q;
+        if (k < nv) {
+            int p = pos[q];
+            if (in[q]) {
+                P.X[p] = x[q]; P.Y[p] = y[q];
+                P.A[p] = la[q]; P.B[p] = lb[q]; P.C[p] = lc[q]; P.L[p] = ll[q];
+                p++;
+            }
+            if (in[q] != inn[q]) {
+                P.X[p] = ix[q]; P.Y[p] = iy[q];
+                if (in[q]) { P.A[p] = a; P.B[p] = b; P.C[p] = c; P.L[p] = lab; }
+                else { P.A[p] = la[q]; P.B[p] = lb[q]; P.C[p] = lc[q]; P.L[p] = ll[q]; }
+            }
+        }
+    }
+    __syncwarp();
+    return base;
+}
+
+// Clip by every candidate of the chunk (one per lane, j < 0 = none) that cuts
+// the polygon, nearest site first.  A candidate that does not cut the polygon
+// can never cut a later (smaller) one and is dropped for good.
+template <int MAXV>
+__device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, double2 si, double wi,
+                          const double *__restrict__ wt, int lane, int &status)
+{
+    bool act = j >= 0;
+    double a = 0.0, b = 0.0, c = 0.0, key = INFINITY;
+    if (act) {
+        double2 sj = g.xy[j];
+        a = sj.x - si.x;
+        b = sj.y - si.y;
+        key = a * a + b * b;
+        c = 0.5 * (key - (wt[j] - wi));
+    }
+    while (true) {
+        bool cut = false;
+        if (act) {
+            for (int k = 0; k < nv; k++) {
+                if (side(a, b, c, P.X[k], P.Y[k]) > 0.0) { cut = true; break; }
+            }
+            if (!cut) act = false;
+        }
+        unsigned mask = __ballot_sync(FULLMASK, cut);
+        if (mask == 0u) break;
+        double kk = cut ? key : INFINITY;
+        int bl = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ok = __shfl_xor_sync(FULLMASK, kk, o);
+            int ol = __shfl_xor_sync(FULLMASK, bl, o);
+            if (ok < kk || (ok == kk && ol < bl)) { kk = ok; bl = ol; }
+        }
+        double A = __shfl_sync(FULLMASK, a, bl);
+        double B = __shfl_sync(FULLMASK, b, bl);
+        double Cc = __shfl_sync(FULLMASK, c, bl);
+        int J = __shfl_sync(FULLMASK, j, bl);
+        int r = clip_poly<MAXV>(P, nv, A, B, Cc, J, lane);
+        if (r < 0) { status = 1; return nv; }
+        nv = r;
+        if (lane == bl) act = false;
+        if (nv == 0) return 0;
+    }
+    return nv;
+}
+
+// Can no site of `node` beat site i anywhere on the current polygon?
+template <int MAXV>
+__device__ __forceinline__ bool node_excluded(const WarpPoly<MAXV> &P, int nv, const CotGeo &g, int node,
+                                              double2 si, double halfs2w)
+{
+    double4 st = g.tstat[node];
+    if (st.w <= 0.0) return true;
+    double4 dy = g.tdyn[node];
+    double qx = si.x - dy.x, qy = si.y - dy.y;
+    double gx = st.x - si.x, gy = st.y - si.y;
+    double K = dy.z + qx * st.x + qy * st.y - halfs2w;
+    double r2 = st.z * st.z;
+    for (int k = 0; k < nv; k++) {
+        double x = P.X[k], y = P.Y[k];
+        double R = -g.margin - K - (x * gx + y * gy);
+        if (R <= 0.0) return false;
+        double ux = qx + x, uy = qy + y;
+        if (r2 * (ux * ux + uy * uy) >= R * R) return false;
+    }
+    return true;
+}
+
+// Green terms of one directed segment in pixel-local coordinates.
+struct Mom { double A, Ia, Ib, I2; };
+
+__device__ __forceinline__ void seg_terms(double a0, double b0, double a1, double b1, Mom &m)
+{
+    double db = b1 - b0;
+    m.A += db * (a0 + a1) * 0.5;
+    m.Ia += db * (a0 * a0 + a0 * a1 + a1 * a1) * (1.0 / 6.0);
+    m.Ib += db * (2.0 * a0 * b0 + a0 * b1 + a1 * b0 + 2.0 * a1 * b1) * (1.0 / 6.0);
+    double c3 = (a0 * a0 * a0 + a0 * a0 * a1 + a0 * a1 * a1 + a1 * a1 * a1) * (1.0 / 12.0);
+    double cb = (a0 * (3.0 * b0 * b0 + 2.0 * b0 * b1 + b1 * b1) + a1 * (b0 * b0 + 2.0 * b0 * b1 + 3.0 * b1 * b1)) *
+                (1.0 / 12.0);
+    m.I2 += db * (c3 + cb);
+}
+
+// Vertical segment at a from b0 to b1.
+__device__ __forceinline__ void vside_terms(double a, double b0, double b1, Mom &m)
+{
+    double db = b1 - b0;
+    m.A += a * db;
+    m.Ia += 0.5 * a * a * db;
+    m.Ib += 0.5 * a * (b1 * b1 - b0 * b0);
+    m.I2 += a * a * a * (1.0 / 3.0) * db + a * (b1 * b1 * b1 - b0 * b0 * b0) * (1.0 / 3.0);
+}
+
+// Section [lo, hi] of the polygon at the vertical line x (lo > hi: empty).
+template <int MAXV>
+__device__ __forceinline__ void section_at(const WarpPoly<MAXV> &P, int nv, double x, double &lo, double &hi)
+{
+    lo = INFINITY;
+    hi = -INFINITY;
+    for (int k = 0; k < nv; k++) {
+        int kn = (k + 1 == nv) ? 0 : k + 1;
+        double px = P.X[k], py = P.Y[k], qx = P.X[kn], qy = P.Y[kn];
+        if (px == qx) {
+            if (px == x) {
+                lo = fmin(lo, fmin(py, qy));
+                hi = fmax(hi, fmax(py, qy));
+            }
+            continue;
+        }
+        double mn = fmin(px, qx), mx = fmax(px, qx);
+        if (x < mn || x > mx) continue;
+        double yy = (x == px) ? py : (x == qx) ? qy : py + (x - px) * (qy - py) / (qx - px);
+        lo = fmin(lo, yy);
+        hi = fmax(hi, yy);
+    }
+}
+
+struct CellAcc { double mu, S, Mt, Mx, My; };
+
+// Integrate the density over the cell (polygon relative to site si).
+template <int MAXV>
+__device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, double2 si, int lane)
+{
+    CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
+    for (int k = lane; k < nv; k += 32) {
+        mnx = fmin(mnx, P.X[k]); mxx = fmax(mxx, P.X[k]);
+        mny = fmin(mny, P.Y[k]); mxy = fmax(mxy, P.Y[k]);
+    }
+    mnx = warp_min(mnx); mxx = warp_max(mxx); mny = warp_min(mny); mxy = warp_max(mxy);
+    // pixel range of the bounding box (basic_function.cuh:791-799)
+    int lx = (int)floor((si.x + mnx - g.pd[0]) / g.xs);
+    int ly = (int)floor((si.y + mny - g.pd[2]) / g.ys);
+    int hx = (int)floor((si.x + mxx - g.pd[0]) / g.xs) + 1;
+    int hy = (int)floor((si.y + mxy - g.pd[2]) / g.ys) + 1;
+    lx = lx > 0 ? lx : 0;
+    ly = ly > 0 ? ly : 0;
+    hx = hx < g.nx ? hx : g.nx;
+    hy = hy < g.ny ? hy : g.ny;
+    if (hx <= lx || hy <= ly) return acc;
+    const double pminx = mnx, pmaxx = mxx;
+    double mu = 0.0, S = 0.0, Mt = 0.0, Mx = 0.0, My = 0.0;
+    for (int cx0 = lx; cx0 < hx; cx0 += 32) {
+        int cw = min(32, hx - cx0);
+        // column lines cx0 .. cx0+cw
+        for (int c = lane; c <= cw; c += 32) {
+            double xl = (double)(cx0 + c) * g.xs + g.pd[0] - si.x;
+            double lo, hi;
+            section_at<MAXV>(P, nv, xl, lo, hi);
+            P.elo[c] = lo;
+            P.ehi[c] = hi;
+            P.rv[c] = (pminx <= xl && xl < pmaxx) ? 1 : 0;  // right limit (left side of a pixel)
+            P.lv[c] = (pminx < xl && xl <= pmaxx) ? 1 : 0;  // left limit (right side of a pixel)
+        }
+        __syncwarp();
+        // y-range of the cell inside each column strip
+        for (int c = lane; c < cw; c += 32) {
+            double xl = (double)(cx0 + c) * g.xs + g.pd[0] - si.x;
+            double xr = (double)(cx0 + c + 1) * g.xs + g.pd[0] - si.x;
+            double lo = INFINITY, hi = -INFINITY;
+            if (P.rv[c]) { lo = fmin(lo, P.elo[c]); hi = fmax(hi, P.ehi[c]); }
+            if (P.lv[c + 1]) { lo = fmin(lo, P.elo[c + 1]); hi = fmax(hi, P.ehi[c + 1]); }
+            for (int k = 0; k < nv; k++) {
+                double vx = P.X[k];
+                if (vx > xl && vx < xr) { lo = fmin(lo, P.Y[k]); hi = fmax(hi, P.Y[k]); }
+            }
+            P.slo[c] = lo;
+            P.shi[c] = hi;
+        }
+        __syncwarp();
+        int rows = hy - ly;
+        int npx = cw * rows;
+        for (int p = lane; p < npx; p += 32) {
+            int c = p % cw, r = p / cw;
+            int ix = cx0 + c, iy = ly + r;
+            // pixel box exactly as basic_function.cuh:806-809, relative to the site
+            double x0 = (double)ix * g.xs + g.pd[0] - si.x;
+            double x1 = (double)(ix + 1) * g.xs + g.pd[0] - si.x;
+            double y0 = (double)iy * g.ys + g.pd[2] - si.y;
+            double y1 = (double)(iy + 1) * g.ys + g.pd[2] - si.y;
+            if (!(P.shi[c] > y0 && P.slo[c] < y1)) continue;
+            double xc = 0.5 * (x0 + x1), yc = 0.5 * (y0 + y1);
+            double hxp = 0.5 * (x1 - x0), hyp = 0.5 * (y1 - y0);
+            Mom m = {0.0, 0.0, 0.0, 0.0};
+            bool full = P.rv[c] && P.lv[c + 1] && P.elo[c] <= y0 && P.ehi[c] >= y1 && P.elo[c + 1] <= y0 &&
+                        P.ehi[c + 1] >= y1;
+            if (full) {
+                m.A = 4.0 * hxp * hyp;
+                m.I2 = m.A * (hxp * hxp + hyp * hyp) * (1.0 / 3.0);
+            } else {
+                for (int k = 0; k < nv; k++) {
+                    int kn = (k + 1 == nv) ? 0 : k + 1;
+                    double px = P.X[k], py = P.Y[k], qx = P.X[kn], qy = P.Y[kn];
+                    if (px == qx && (px == x0 || px == x1)) continue;  // counted by the pixel side
+                    if (fmax(px, qx) < x0 || fmin(px, qx) > x1 || fmax(py, qy) < y0 || fmin(py, qy) > y1) continue;
+                    // Liang-Barsky against the pixel box
+                    double dx = qx - px, dy = qy - py, t0 = 0.0, t1 = 1.0;
+                    bool ok = true;
+                    double pp[4] = {-dx, dx, -dy, dy};
+                    double qq[4] = {px - x0, x1 - px, py - y0, y1 - py};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        if (pp[e] == 0.0) {
+                            if (qq[e] < 0.0) ok = false;
+                        } else {
+                            double t = qq[e] / pp[e];
+                            if (pp[e] < 0.0) { if (t > t0) t0 = t; }
+                            else { if (t < t1) t1 = t; }
+                        }
+                    }
+                    if (!ok || !(t0 < t1)) continue;
+                    double ax0 = (t0 == 0.0 ? px : px + t0 * dx) - xc;
+                    double by0 = (t0 == 0.0 ? py : py + t0 * dy) - yc;
+                    double ax1 = (t1 == 1.0 ? qx : px + t1 * dx) - xc;
+                    double by1 = (t1 == 1.0 ? qy : py + t1 * dy) - yc;
+                    seg_terms(ax0, by0, ax1, by1, m);
+                }
+                if (P.lv[c + 1]) {  // right side, upwards
+                    double b0 = fmax(P.elo[c + 1], y0), b1 = fmin(P.ehi[c + 1], y1);
+                    if (b1 > b0) vside_terms(x1 - xc, b0 - yc, b1 - yc, m);
+                }
+                if (P.rv[c]) {      // left side, downwards
+                    double b0 = fmax(P.elo[c], y0), b1 = fmin(P.ehi[c], y1);
+                    if (b1 > b0) vside_terms(x0 - xc, b1 - yc, b0 - yc, m);
+                }
+            }
+            if (!(m.A > 0.0)) continue;
+            double rho = g.rho[ix + iy * g.nx];
+            mu += rho * m.A;
+            S += rho * (m.A * (xc * xc + yc * yc) + 2.0 * (xc * m.Ia + yc * m.Ib) + m.I2);
+            if (m.A > 1e-10) {  // compute_center skips tiny pieces (basic_function.cuh:1153)
+                Mt += rho * m.A;
+                Mx += rho * (m.A * xc + m.Ia);
+                My += rho * (m.A * yc + m.Ib);
+            }
+        }
+        __syncwarp();
+    }
+    acc.mu = warp_sum(mu);
+    acc.S = warp_sum(S);
+    acc.Mt = warp_sum(Mt);
+    acc.Mx = warp_sum(Mx);
+    acc.My = warp_sum(My);
+    return acc;
+}
+
+// Plain area centroid of the polygon (relative to the site).
+template <int MAXV>
+__device__ void poly_centroid(const WarpPoly<MAXV> &P, int nv, int lane, double &cx, double &cy)
+{
+    double a = 0.0, mx = 0.0, my = 0.0;
+    for (int k = lane; k < nv; k += 32) {
+        int kn = (k + 1 == nv) ? 0 : k + 1;
+        double x0 = P.X[k], y0 = P.Y[k], x1 = P.X[kn], y1 = P.Y[kn];
+        double cr = x0 * y1 - x1 * y0;
+        a += cr;
+        mx += (x0 + x1) * cr;
+        my += (y0 + y1) * cr;
+    }
+    a = warp_sum(a);
+    mx = warp_sum(mx);
+    my = warp_sum(my);
+    cx = a != 0.0 ? mx / (3.0 * a) : 0.0;
+    cy = a != 0.0 ? my / (3.0 * a) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// the cell kernel
+// ---------------------------------------------------------------------------
+// mode 0: every cell (grid-stride); mode 1: the cells listed in ovf_list.
+template <int MAXV>
+__global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    WarpPoly<MAXV> &P = reinterpret_cast<WarpPoly<MAXV> *>(smem_raw)[wib];
+    const double *__restrict__ wt = a.wt;
+
+    int total = (mode == 0) ? g.n : *a.ovf_count;
+    for (int idx = blockIdx.x * wpb + wib; idx < total; idx += gridDim.x * wpb) {
+        const int i = (mode == 0) ? idx : a.ovf_list[idx];
+        const double2 si = g.xy[i];
+        const double wi = wt[i];
+        int status = 0;
+        // domain rectangle, CCW, relative to the site
+        int nv = 4;
+        if (lane == 0) {
+            double x0 = g.pd[0] - si.x, x1 = g.pd[1] - si.x, y0 = g.pd[2] - si.y, y1 = g.pd[3] - si.y;
+            P.X[0] = x0; P.Y[0] = y0; P.A[0] = 0.0;  P.B[0] = -1.0; P.C[0] = -y0; P.L[0] = -1;
+            P.X[1] = x1; P.Y[1] = y0; P.A[1] = 1.0;  P.B[1] = 0.0;  P.C[1] = x1;  P.L[1] = -2;
+            P.X[2] = x1; P.Y[2] = y1; P.A[2] = 0.0;  P.B[2] = 1.0;  P.C[2] = y1;  P.L[2] = -3;
+            P.X[3] = x0; P.Y[3] = y1; P.A[3] = -1.0; P.B[3] = 0.0;  P.C[3] = -x0; P.L[3] = -4;
+        }
+        __syncwarp();
+        // ---- 1. neighbour window ------------------------------------------------
+        const int bi = g.sbucket[i];
+        const int bu = bi % g.bx, bv = bi / g.bx;
+        {
+            int bcnt = 0, bst = 0;
+            if (lane < 9) {
+                // own bucket, then the 4 edge neighbours, then the corners
+                const int tdu[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+                const int tdv[9] = {0, 0, 0, 1, -1, 1, 1, -1, -1};
+                int u = bu + tdu[lane], v = bv + tdv[lane];
+                if (u >= 0 && u < g.bx && v >= 0 && v < g.by) {
+                    int b = u + v * g.bx;
+                    bst = g.bstart[b];
+                    bcnt = g.bstart[b + 1] - bst;
+                }
+            }
+            int inc = warp_incl_scan(bcnt, lane);
+            int tot = __shfl_sync(FULLMASK, inc, 31);
+            for (int base = 0; base < tot && nv > 0 && status == 0; base += 32) {
+                int t = base + lane, j = -1;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    int ik = __shfl_sync(FULLMASK, inc, k);
+                    int sk = __shfl_sync(FULLMASK, bst, k);
+                    int ck = __shfl_sync(FULLMASK, bcnt, k);
+                    if (j < 0 && t < tot && t < ik) j = sk + (t - (ik - ck));
+                }
+                if (j == i) j = -1;
+                nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status);
+            }
+        }
+        // ---- 2. certificate over the bound tree --------------------------------
+        const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
+        bool brute = false;
+        if (nv > 0 && status == 0 && g.nlev > 0) {
+            int top = g.nlev - 1;
+            int ncur = g.lev_w[top] * g.lev_h[top];
+            if (ncur > COT_FRMAX) brute = true;
+            int cur = 0;
+            if (!brute) {
+                for (int q = lane; q < ncur; q += 32) P.fr[0][q] = q;
+                __syncwarp();
+            }
+            for (int L = top; L >= 0 && !brute && nv > 0 && status == 0; L--) {
+                int nnext = 0;
+                const int off = g.lev_off[L], W = g.lev_w[L];
+                for (int base = 0; base < ncur; base += 32) {
+                    int q = (base + lane < ncur) ? P.fr[cur][base + lane] : -1;
+                    bool keep = false;
+                    if (q >= 0) {
+                        if (L == 0) {
+                            int u = q % W, v = q / W;
+                            bool inwin = abs(u - bu) <= COT_WIN && abs(v - bv) <= COT_WIN;
+                            keep = !inwin && !node_excluded<MAXV>(P, nv, g, off + q, si, halfs2w);
+                        } else {
+                            keep = !node_excluded<MAXV>(P, nv, g, off + q, si, halfs2w);
+                        }
+                    }
+                    if (L == 0) {
+                        unsigned m = __ballot_sync(FULLMASK, keep);
+                        int pos = nnext + __popc(m & ((1u << lane) - 1u));
+                        int cnt = __popc(m);
+                        if (nnext + cnt > COT_FRMAX) { brute = true; break; }
+                        if (keep) P.fr[1 - cur][pos] = q;
+                        nnext += cnt;
+                    } else {
+                        int chc = 0;
+                        int u = 0, v = 0, cw = g.lev_w[L - 1], ch = g.lev_h[L - 1];
+                        if (keep) {
+                            u = q % W; v = q / W;
+                            for (int bb = 0; bb < 2; bb++)
+                                for (int aa = 0; aa < 2; aa++)
+                                    if (2 * u + aa < cw && 2 * v + bb < ch) chc++;
+                        }
+                        int inc = warp_incl_scan(chc, lane);
+                        int cnt = __shfl_sync(FULLMASK, inc, 31);
+                        if (nnext + cnt > COT_FRMAX) { brute = true; break; }
+                        int pos = nnext + inc - chc;
+                        if (keep) {
+                            for (int bb = 0; bb < 2; bb++)
+                                for (int aa = 0; aa < 2; aa++)
+                                    if (2 * u + aa < cw && 2 * v + bb < ch) P.fr[1 - cur][pos++] = (2 * u + aa) + (2 * v + bb) * cw;
+                        }
+                        nnext += cnt;
+                    }
+                }
+                __syncwarp();
+                cur = 1 - cur;
+                ncur = nnext;
+                if (brute) break;
+                if (L == 0) {
+                    // clip by the sites of every leaf that survived
+                    for (int li = 0; li < ncur && nv > 0 && status == 0; li++) {
+                        int b = P.fr[cur][li];
+                        int s0 = g.bstart[b], s1 = g.bstart[b + 1];
+                        for (int base = s0; base < s1 && nv > 0 && status == 0; base += 32) {
+                            int j = base + lane < s1 ? base + lane : -1;
+                            nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status);
+                        }
+                    }
+                }
+            }
+        }
+        if (brute && nv > 0 && status == 0) {
+            // frontier overflow: test every bucket against the current polygon
+            const int nb = g.bx * g.by;
+            for (int base = 0; base < nb && nv > 0 && status == 0; base += 32) {
+                int b = base + lane;
+                bool keep = false;
+                if (b < nb) {
+                    int u = b % g.bx, v = b / g.bx;
+                    bool inwin = abs(u - bu) <= COT_WIN && abs(v - bv) <= COT_WIN;
+                    keep = !inwin && !node_excluded<MAXV>(P, nv, g, b, si, halfs2w);
+                }
+                unsigned m = __ballot_sync(FULLMASK, keep);
+                while (m != 0u && nv > 0 && status == 0) {
+                    int l = __ffs(m) - 1;
+                    m &= m - 1u;
+                    int bb = base + l;
+                    int s0 = g.bstart[bb], s1 = g.bstart[bb + 1];
+                    for (int sb = s0; sb < s1 && nv > 0 && status == 0; sb += 32) {
+                        int j = sb + lane < s1 ? sb + lane : -1;
+                        nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status);
+                    }
+                }
+            }
+        }
+        if (status != 0) {
+            // ring above MAXV: hand the cell to the large-capacity pass
+            if (mode == 0 && lane == 0) {
+                int slot = atomicAdd(a.ovf_count, 1);
+                a.ovf_list[slot] = i;
+                a.nv[i] = MAXV + 1;
+            } else if (lane == 0) {
+                a.nv[i] = MAXV + 1;
+                a.mu[i] = 0.0;
+                a.fc[i] = 0.0;
+            }
+            __syncwarp();
+            continue;
+        }
+        // ---- 3. integrate the density over the cell --------------------------
+        CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (nv >= 3) acc = integrate_cell<MAXV>(P, nv, g, si, lane);
+        double pcx = 0.0, pcy = 0.0;
+        if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid<MAXV>(P, nv, lane, pcx, pcy);
+        if (a.ring_xy != nullptr) {
+            for (int k = lane; k < nv && k < a.ring_cap; k += 32) {
+                a.ring_xy[2 * ((size_t)i * a.ring_cap + k)] = si.x + P.X[k];
+                a.ring_xy[2 * ((size_t)i * a.ring_cap + k) + 1] = si.y + P.Y[k];
+                a.ring_lab[(size_t)i * a.ring_cap + k] = P.L[k];
+            }
+        }
+        if (lane == 0) {
+            a.mu[i] = acc.mu;
+            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941)
+            a.fc[i] = -wi * g.nu[i] - (acc.S - wi * acc.mu);
+            a.nv[i] = nv;
+            if (a.cen != nullptr) {
+                bool ex = nv >= 3;
+                a.exist[i] = ex ? 1 : 0;
+                double cx = si.x, cy = si.y;
+                if (ex) {
+                    if (a.weighted && acc.Mt != 0.0) {
+                        cx = si.x + acc.Mx / acc.Mt;
+                        cy = si.y + acc.My / acc.Mt;
+                    } else {
+                        cx = si.x + pcx;
+                        cy = si.y + pcy;
+                    }
+                }
+                a.cen[2 * i] = cx;
+                a.cen[2 * i + 1] = cy;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+static size_t cells_smem(int maxv, int warps)
+{
+    switch (maxv) {
+    case 64: return sizeof(WarpPoly<64>) * (size_t)warps;
+    default: return sizeof(WarpPoly<256>) * (size_t)warps;
+    }
+}
+
+void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms, cudaStream_t s)
+{
+    int nb = g.bx * g.by;
+    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar);
+    k_bucket_bound<<<(nb + 127) / 128, 128, 0, s>>>(g, a.wt, a.phibar);
+    for (int L = 1; L < g.nlev; L++) {
+        int cnt = g.lev_w[L] * g.lev_h[L];
+        k_tree_level<<<(cnt + 127) / 128, 128, 0, s>>>(g, L);
+    }
+    cudaMemsetAsync(a.ovf_count, 0, sizeof(int), s);
+    int wpb = warps_per_block > 0 ? warps_per_block : 4;
+    int blocks = (g.n + wpb - 1) / wpb;
+    size_t sm = cells_smem(64, wpb);
+    k_cells<64><<<blocks, 32 * wpb, sm, s>>>(g, a, 0);
+    // overflowing cells (rare): one warp per block, 256-vertex rings
+    int ob = num_sms > 0 ? num_sms : 148;
+    k_cells<256><<<ob, 32, cells_smem(256, 1), s>>>(g, a, 1);
+}
+
+// Dynamic shared memory above 48 KB needs an opt-in per kernel.
+void configure_cells_kernels()
+{
+    cudaFuncSetAttribute(k_cells<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(64, 8));
+    cudaFuncSetAttribute(k_cells<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(256, 1));
+}
+
+}  // namespace cot

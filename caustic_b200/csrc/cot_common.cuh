@@ -1,0 +1,144 @@
+// Internal types shared by the solver's CUDA translation units.
+//
+// Data layout in HBM (one problem per handle):
+//   sites     double2 xy[n]      sorted by neighbour bucket, then input index
+//   masses    double  nu[n]      same order
+//   buckets   int     bstart[nb+1]  CSR into the sorted sites, row-major
+//             (bucket (u,v) = u + v*bx) over the sites' bounding box
+//   tree      double4 tstat[nodes] {mean x, mean y, radius, count} (static)
+//             double4 tdyn[nodes]  {cx, cy, A, 0} plane bound (per evaluation)
+//             level 0 = the buckets, each higher level merges 2x2 nodes
+//   density   double  rho[nx*ny] density per unit area, rho[ix + iy*nx]
+//
+// Every per-site vector the solver keeps (w, mu, L-BFGS history) is in the
+// sorted order; the C ABI permutes at the boundary.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define COT_MAX_LEVELS 24
+#define COT_MAX_HIST 32
+#define COT_BASIS (2 * COT_MAX_HIST + 1)
+
+// Static geometry, passed by value to the kernels.
+struct CotGeo {
+    int n;                 // sites
+    const double2 *xy;     // sorted sites
+    const double *nu;      // sorted masses
+    const int *bstart;     // bucket CSR, nb + 1 entries
+    const int *sbucket;    // bucket of each sorted site
+    int bx, by;            // bucket grid
+    double ox, oy;         // bucket grid origin
+    double ihx, ihy;       // inverse bucket extent
+    int nlev;              // tree levels (level 0 = buckets)
+    int lev_off[COT_MAX_LEVELS];
+    int lev_w[COT_MAX_LEVELS];
+    int lev_h[COT_MAX_LEVELS];
+    const double4 *tstat;  // {mx, my, r, count}
+    double4 *tdyn;         // {cx, cy, A, 0}
+    const double *rho;     // density per unit area
+    int nx, ny;            // pixels along x, along y
+    double pd[4];          // proj_domain {xmin, xmax, ymin, ymax}
+    double xs, ys;         // pixel extent (reference x_step, y_step)
+    double margin;         // safety margin of the plane-bound exclusion test
+};
+
+// Per-evaluation scalar results (written by the reduction's last block).
+struct CotEvalOut {
+    double f;          // sum_i f_i
+    double gtd;        // sum_i (mu_i - nu_i) d_i   (0 without a direction)
+    double maxrel;     // max_i |mu_i - nu_i| / nu_i
+    double gnorm2;     // sum_i (mu_i - nu_i)^2
+    int empty;         // cells with mu_i == 0
+    int overflow;      // cells above the ring capacity / threshold
+    int maxnv;         // largest ring
+    int pad;
+};
+
+// Solver state kept on the device; every control decision is taken by one
+// device thread so that the loop can run without host round trips.
+struct CotSolver {
+    // control block: the host reads these first 16 ints after each trial
+    int ls_active;       // 1 while line-search trials remain
+    int accepted;        // 1 when the last trial was accepted
+    int done;
+    int converged;
+    int failed;
+    int iter, evals, restarts, ring_rejects;
+    int k;               // stored pairs (loop_iter of the reference)
+    int restart;         // reference's restart flag
+    int trials;
+    int final_eval;      // Wolfe: the pending trial re-evaluates lo
+    int ctl_pad[3];
+    // options
+    int mode;            // COT_SOLVE_*
+    int m;               // history
+    int max_ls;
+    int max_iter;
+    int max_ring;
+    int opt_pad;
+    double c1, c2, t0, tol;
+    double H0;
+    double rho[COT_MAX_HIST];
+    double alpha[COT_MAX_HIST];
+    double delta[COT_BASIS];            // direction = sum delta_j * basis_j
+    double G[COT_BASIS * COT_BASIS];    // Gram matrix of the basis
+    // current point
+    double f, gd;
+    double maxrel, gnorm2;
+    int empty;
+    int empty_stale;
+    double gnorm_stale;  // ||g|| taken at the start of the iteration
+    // line search
+    double t, lo, hi, f_lo;
+    // last trial
+    CotEvalOut last;
+};
+
+#define COT_CUDA_TRY(expr)                                                                 \
+    do {                                                                                   \
+        cudaError_t e__ = (expr);                                                          \
+        if (e__ != cudaSuccess) return cot::fail(h, COT_ECUDA, #expr, cudaGetErrorString(e__)); \
+    } while (0)
+
+namespace cot {
+
+// Launchers implemented in cot_cells.cu.
+struct CellsArgs {
+    const double *w;       // weights (base point)
+    const double *d;       // direction (nullable)
+    const double *tptr;    // device scalar step (nullable => 0)
+    double *wt;            // trial weights out
+    double *phibar;        // per bucket scratch
+    double *mu;            // per cell mass out
+    double *fc;            // per cell objective out
+    int *nv;               // per cell ring size out
+    int *ovf_list;         // cells to redo with the large ring capacity
+    int *ovf_count;        // device counter
+    double *cen;           // centroids (nullable)
+    unsigned char *exist;  // exist flags (nullable)
+    int weighted;          // centroid flavour
+    double *ring_xy;       // optional fixed-stride ring dump (nullable)
+    int *ring_lab;
+    int ring_cap;
+};
+
+void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms,
+                 cudaStream_t s);
+void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const int *nv,
+                   const double *wt, const double *d, int max_ring, double *partials,
+                   unsigned int *ticket, CotEvalOut *out, CotSolver *solver, cudaStream_t s);
+int reduce_blocks(int n);
+
+// Launchers implemented in cot_solver.cu.
+void launch_begin_iteration(CotSolver *S, cudaStream_t s);
+void launch_direction(const CotGeo &g, const CotSolver *S, const double *Sv, const double *Yv,
+                      const double *mu, double *d, cudaStream_t s);
+void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double *w,
+                   const double *wt, double *mu, const double *mut, const double *d,
+                   double *partials, unsigned int *ticket, int initial, cudaStream_t s);
+void launch_reject(CotSolver *S, cudaStream_t s);
+void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, cudaStream_t s);
+void configure_cells_kernels();
+
+}  // namespace cot

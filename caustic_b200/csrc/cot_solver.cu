@@ -1,0 +1,458 @@
+// Device-resident L-BFGS for the dual weights.
+//
+// Replaces the solver loop of direct_ot (ot_op.cuh:289-537).  The reference
+// runs the two-loop recursion with one kernel per vector operation and moves
+// every dot product to the host (2m+1 device->host copies of N doubles per
+// iteration, ot_op.cuh:298-337).  Here the two-loop runs on the Gram matrix of
+// the basis {s_0..s_{m-1}, y_0..y_{m-1}, g} (the vector-free form of the
+// recursion): after each accepted step one pass over N computes the 5m+1 new
+// dot products, one device thread runs the recursion on the (2m+1)^2 matrix,
+// and one pass forms d = sum_j delta_j b_j.  Every reduction is a fixed-order
+// tree (per-block partials summed in block order by the last block), so a
+// solve is bit-reproducible run to run.  Line-search decisions are taken by
+// one device thread as well; the host only reads a flag.
+#include "cot_common.cuh"
+#include "../../include/causticot.h"
+#include <math.h>
+
+namespace cot {
+
+#define FULLMASK 0xffffffffu
+#define RED_THREADS 256
+#define RED_VALS 8
+
+int reduce_blocks(int n)
+{
+    int b = (n + RED_THREADS * 4 - 1) / (RED_THREADS * 4);
+    if (b < 1) b = 1;
+    if (b > 1024) b = 1024;
+    return b;
+}
+
+__device__ __forceinline__ double wsum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+    return v;
+}
+__device__ __forceinline__ double wmax(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULLMASK, v, o));
+    return v;
+}
+
+// Fixed-order block reduction of one value (sum or max).  All threads call it.
+template <bool MAX>
+__device__ double block_reduce(double v, double *sh)
+{
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = MAX ? wmax(v) : wsum(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = MAX ? -INFINITY : 0.0;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < nw; k++) r = MAX ? fmax(r, sh[k]) : r + sh[k];
+        sh[32] = r;
+    }
+    __syncthreads();
+    return sh[32];
+}
+
+// Line-search decision for the trial just reduced (one thread).
+__device__ void ls_decide(CotSolver *S, const CotEvalOut &o)
+{
+    S->evals++;
+    S->last = o;
+    S->accepted = 0;
+    if (S->mode == COT_SOLVE_REFERENCE) {
+        // ot_op.cuh:360-426
+        if (o.overflow > 0) {
+            S->ring_rejects++;
+            S->t *= 0.5;
+        } else if (o.f < S->f) {
+            S->accepted = 1;
+            S->ls_active = 0;
+            return;
+        } else {
+            S->t *= 0.5;
+        }
+        if (S->t <= 1e-4 * S->t0) S->ls_active = 0;  // restart
+        return;
+    }
+    // strong Wolfe: bracket by doubling, zoom by bisection
+    if (S->final_eval) {
+        S->accepted = 1;
+        S->ls_active = 0;
+        return;
+    }
+    double t = S->t;
+    bool bad = o.overflow > 0;
+    if (bad) S->ring_rejects++;
+    if (bad || !(o.f <= S->f + S->c1 * t * S->gd) || o.f >= S->f_lo) {
+        S->hi = t;
+    } else if (fabs(o.gtd) <= S->c2 * fabs(S->gd)) {
+        S->accepted = 1;
+        S->ls_active = 0;
+        return;
+    } else if (o.gtd > 0.0) {
+        S->hi = t;
+    } else {
+        S->lo = t;
+        S->f_lo = o.f;
+    }
+    S->trials++;
+    if (S->trials >= S->max_ls) {
+        if (S->lo > 0.0) {
+            S->t = S->lo;
+            S->final_eval = 1;
+        } else {
+            S->ls_active = 0;  // failed
+        }
+        return;
+    }
+    S->t = isinf(S->hi) ? 2.0 * t : 0.5 * (S->lo + S->hi);
+}
+
+// One pass over the cells: objective, gradient statistics, directional
+// derivative; the last block finishes the sums and (in a solve) decides.
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_eval(int n, const double *__restrict__ mu,
+                                                            const double *__restrict__ fc, const int *__restrict__ nv,
+                                                            const double *__restrict__ nu, const double *__restrict__ d,
+                                                            int max_ring, double *partials, unsigned int *ticket,
+                                                            CotEvalOut *out, CotSolver *S)
+{
+    __shared__ double sh[33];
+    __shared__ bool last;
+    if (S != nullptr && (S->done || !S->ls_active)) return;
+    double f = 0.0, gtd = 0.0, mx = 0.0, gn = 0.0, emp = 0.0, ovf = 0.0, mnv = 0.0;
+    int per = (n + gridDim.x - 1) / gridDim.x;
+    int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        double g = mu[i] - nu[i];
+        f += fc[i];
+        if (d != nullptr) gtd += g * d[i];
+        double rel = nu[i] > 0.0 ? fabs(g) / nu[i] : (g != 0.0 ? INFINITY : 0.0);
+        mx = fmax(mx, rel);
+        gn += g * g;
+        emp += (mu[i] == 0.0) ? 1.0 : 0.0;
+        ovf += (nv[i] > max_ring) ? 1.0 : 0.0;
+        mnv = fmax(mnv, (double)nv[i]);
+    }
+    double v[RED_VALS];
+    v[0] = block_reduce<false>(f, sh);
+    v[1] = block_reduce<false>(gtd, sh);
+    v[2] = block_reduce<true>(mx, sh);
+    v[3] = block_reduce<false>(gn, sh);
+    v[4] = block_reduce<false>(emp, sh);
+    v[5] = block_reduce<false>(ovf, sh);
+    v[6] = block_reduce<true>(mnv, sh);
+    v[7] = 0.0;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < RED_VALS; k++) partials[blockIdx.x * RED_VALS + k] = v[k];
+        __threadfence();
+        unsigned int tk = atomicAdd(ticket, 1u);
+        last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        volatile double *p = partials;
+        double r[RED_VALS] = {0, 0, 0, 0, 0, 0, 0, 0};
+        r[2] = 0.0;
+        r[6] = 0.0;
+        for (unsigned b = 0; b < gridDim.x; b++) {
+            r[0] += p[b * RED_VALS + 0];
+            r[1] += p[b * RED_VALS + 1];
+            r[2] = fmax(r[2], p[b * RED_VALS + 2]);
+            r[3] += p[b * RED_VALS + 3];
+            r[4] += p[b * RED_VALS + 4];
+            r[5] += p[b * RED_VALS + 5];
+            r[6] = fmax(r[6], p[b * RED_VALS + 6]);
+        }
+        CotEvalOut o;
+        o.f = r[0];
+        o.gtd = r[1];
+        o.maxrel = r[2];
+        o.gnorm2 = r[3];
+        o.empty = (int)r[4];
+        o.overflow = (int)r[5];
+        o.maxnv = (int)r[6];
+        o.pad = 0;
+        *out = o;
+        *ticket = 0u;
+        if (S != nullptr) ls_decide(S, o);
+    }
+}
+
+void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const int *nv, const double *wt,
+                   const double *d, int max_ring, double *partials, unsigned int *ticket, CotEvalOut *out,
+                   CotSolver *solver, cudaStream_t s)
+{
+    (void)wt;
+    int nb = reduce_blocks(g.n);
+    k_reduce_eval<<<nb, RED_THREADS, 0, s>>>(g.n, mu, fc, nv, g.nu, d, max_ring, partials, ticket, out, solver);
+}
+
+// ---------------------------------------------------------------------------
+// iteration control (single thread)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double gram_dot(const CotSolver *S, int row, const double *delta)
+{
+    const int B = 2 * S->m + 1;
+    double r = 0.0;
+    for (int c = 0; c < B; c++)
+        if (delta[c] != 0.0) r += S->G[row * COT_BASIS + c] * delta[c];
+    return r;
+}
+
+// Two-loop recursion on the Gram matrix (ot_op.cuh:291-351): delta gives
+// d = sum_j delta_j basis_j; then the descent safeguard.
+__global__ void k_begin_iteration(CotSolver *S)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (S->done) return;
+    const int m = S->m, gi = 2 * m;
+    S->gnorm_stale = sqrt(S->gnorm2);
+    S->empty_stale = S->empty;
+    double *dl = S->delta;
+    for (int c = 0; c < COT_BASIS; c++) dl[c] = 0.0;
+    dl[gi] = -1.0;
+    int cnt = S->k < m ? S->k : m;
+    bool skip = (S->mode == COT_SOLVE_REFERENCE) && S->restart;
+    if (!skip) {
+        for (int i = 1; i <= cnt; i++) {
+            int idx = ((S->k - i) % m + m) % m;
+            S->alpha[idx] = gram_dot(S, idx, dl) * S->rho[idx];
+            dl[m + idx] -= S->alpha[idx];
+        }
+        for (int c = 0; c < COT_BASIS; c++) dl[c] *= S->H0;
+        for (int i = cnt; i > 0; i--) {
+            int idx = ((S->k - i) % m + m) % m;
+            double beta = S->rho[idx] * gram_dot(S, m + idx, dl);
+            dl[idx] += S->alpha[idx] - beta;
+        }
+    }
+    double gd = gram_dot(S, gi, dl);
+    if (!(gd < 0.0)) {
+        for (int c = 0; c < COT_BASIS; c++) dl[c] = 0.0;
+        dl[gi] = -1.0;
+        S->k = 0;
+        S->H0 = 1.0;
+        gd = -S->G[gi * COT_BASIS + gi];
+    }
+    S->gd = gd;
+    S->t = S->t0;
+    S->lo = 0.0;
+    S->hi = INFINITY;
+    S->f_lo = S->f;
+    S->trials = 0;
+    S->ls_active = 1;
+    S->accepted = 0;
+    S->final_eval = 0;
+}
+
+void launch_begin_iteration(CotSolver *S, cudaStream_t s) { k_begin_iteration<<<1, 32, 0, s>>>(S); }
+
+// d = sum_j delta_j basis_j
+__global__ void k_direction(int n, const CotSolver *__restrict__ S, const double *__restrict__ Sv,
+                            const double *__restrict__ Yv, const double *__restrict__ mu,
+                            const double *__restrict__ nu, double *__restrict__ d)
+{
+    if (S->done) return;
+    __shared__ double dl[COT_BASIS];
+    const int m = S->m;
+    for (int c = threadIdx.x; c < 2 * m + 1; c += blockDim.x) dl[c] = S->delta[c];
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double r = dl[2 * m] * (mu[i] - nu[i]);
+        for (int j = 0; j < m; j++) {
+            double a = dl[j], b = dl[m + j];
+            if (a != 0.0) r += a * Sv[(size_t)j * n + i];
+            if (b != 0.0) r += b * Yv[(size_t)j * n + i];
+        }
+        d[i] = r;
+    }
+}
+
+void launch_direction(const CotGeo &g, const CotSolver *S, const double *Sv, const double *Yv, const double *mu,
+                      double *d, cudaStream_t s)
+{
+    int blocks = (g.n + 255) / 256;
+    if (blocks > 4 * 148) blocks = 4 * 148;
+    k_direction<<<blocks, 256, 0, s>>>(g.n, S, Sv, Yv, mu, g.nu, d);
+}
+
+// Accept the trial: s_h = t d, y_h = mu_t - mu, w = w_t, mu = mu_t, then the
+// new Gram entries s_h.y_j, y_h.s_j, y_h.y_j, g.s_j, g.y_j, g.g; the last
+// block updates the matrix, the history scalars (ot_op.cuh:434-466) and the
+// stop test (ot_op.cuh:468-476, 510).
+#define ACC_PER 4
+__global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, double *Sv, double *Yv, double *w,
+                                                       const double *__restrict__ wt, double *mu,
+                                                       const double *__restrict__ mut, const double *__restrict__ nu,
+                                                       const double *__restrict__ d, double *partials,
+                                                       unsigned int *ticket, int initial)
+{
+    __shared__ double sh[33];
+    __shared__ bool last;
+    if (S->done) return;
+    if (!initial && !S->accepted) return;
+    const int m = S->m;
+    const int h = S->k % m;
+    const double t = S->t;
+    const int nvals = 5 * m + 1;
+    int per = (n + gridDim.x - 1) / gridDim.x;
+    int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    // new vectors
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        double mt = mut[i];
+        if (!initial) {
+            Sv[(size_t)h * n + i] = __dmul_rn(t, d[i]);
+            Yv[(size_t)h * n + i] = mt - mu[i];
+            w[i] = wt[i];
+        }
+        mu[i] = mt;
+    }
+    __syncthreads();
+    int cnt = initial ? 0 : (S->k + 1 < m ? S->k + 1 : m);  // slots that hold pairs after this update
+    for (int j = 0; j < m; j++) {
+        double sy = 0.0, ys = 0.0, yy = 0.0, gs = 0.0, gy = 0.0;
+        bool valid = false;
+        if (cnt > 0) {
+            // slot j is valid if it is among the last cnt slots ending at h
+            int age = ((h - j) % m + m) % m;
+            valid = age < cnt;
+        }
+        if (valid) {
+            for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+                double sj = Sv[(size_t)j * n + i], yj = Yv[(size_t)j * n + i];
+                double sn = Sv[(size_t)h * n + i], yn = Yv[(size_t)h * n + i];
+                double g = mu[i] - nu[i];
+                sy += sn * yj;
+                ys += yn * sj;
+                yy += yn * yj;
+                gs += g * sj;
+                gy += g * yj;
+            }
+        }
+        double r0 = block_reduce<false>(sy, sh);
+        double r1 = block_reduce<false>(ys, sh);
+        double r2 = block_reduce<false>(yy, sh);
+        double r3 = block_reduce<false>(gs, sh);
+        double r4 = block_reduce<false>(gy, sh);
+        if (threadIdx.x == 0) {
+            double *pp = partials + (size_t)blockIdx.x * nvals + 5 * j;
+            pp[0] = r0; pp[1] = r1; pp[2] = r2; pp[3] = r3; pp[4] = r4;
+        }
+    }
+    double gg = 0.0;
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        double g = mu[i] - nu[i];
+        gg += g * g;
+    }
+    double rg = block_reduce<false>(gg, sh);
+    if (threadIdx.x == 0) {
+        partials[(size_t)blockIdx.x * nvals + 5 * m] = rg;
+        __threadfence();
+        unsigned int tk = atomicAdd(ticket, 1u);
+        last = (tk == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    volatile double *p = partials;
+    __shared__ double tot[5 * COT_MAX_HIST + 1];
+    for (int v = threadIdx.x; v < nvals; v += blockDim.x) {
+        double r = 0.0;
+        for (unsigned b = 0; b < gridDim.x; b++) r += p[(size_t)b * nvals + v];
+        tot[v] = r;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    *ticket = 0u;
+    const int gi = 2 * m;
+    double *G = S->G;
+    for (int j = 0; j < m; j++) {
+        int age = ((h - j) % m + m) % m;
+        bool valid = cnt > 0 && age < cnt;
+        if (!valid) continue;
+        if (!initial) {
+            G[h * COT_BASIS + (m + j)] = G[(m + j) * COT_BASIS + h] = tot[5 * j + 0];
+            G[(m + h) * COT_BASIS + j] = G[j * COT_BASIS + (m + h)] = tot[5 * j + 1];
+            G[(m + h) * COT_BASIS + (m + j)] = G[(m + j) * COT_BASIS + (m + h)] = tot[5 * j + 2];
+        }
+        G[gi * COT_BASIS + j] = G[j * COT_BASIS + gi] = tot[5 * j + 3];
+        G[gi * COT_BASIS + (m + j)] = G[(m + j) * COT_BASIS + gi] = tot[5 * j + 4];
+    }
+    G[gi * COT_BASIS + gi] = tot[5 * m];
+    // current point
+    S->f = S->last.f;
+    S->maxrel = S->last.maxrel;
+    S->gnorm2 = S->last.gnorm2;
+    S->empty = S->last.empty;
+    if (initial) return;
+    double ys = G[(m + h) * COT_BASIS + h];
+    double yy = G[(m + h) * COT_BASIS + (m + h)];
+    if (S->mode == COT_SOLVE_REFERENCE) {
+        S->rho[h] = 1.0 / ys;
+        S->H0 = (yy > 1e-5) ? ys / yy : 1.0;
+        S->k++;
+        S->restart = 0;
+    } else if (ys > 0.0) {
+        S->rho[h] = 1.0 / ys;
+        S->H0 = ys / yy;
+        S->k++;
+    }
+    S->iter++;
+    if (S->mode == COT_SOLVE_REFERENCE) {
+        if (S->gnorm_stale < S->tol && S->empty_stale == 0) { S->converged = 1; S->done = 1; }
+    } else {
+        if (S->maxrel <= S->tol) { S->converged = 1; S->done = 1; }
+    }
+    if (S->iter >= S->max_iter) S->done = 1;
+}
+
+void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double *w, const double *wt, double *mu,
+                   const double *mut, const double *d, double *partials, unsigned int *ticket, int initial,
+                   cudaStream_t s)
+{
+    int nb = reduce_blocks(g.n);
+    k_accept<<<nb, RED_THREADS, 0, s>>>(g.n, S, Sv, Yv, w, wt, mu, mut, g.nu, d, partials, ticket, initial);
+}
+
+// Line search gave up (ot_op.cuh:413-425): keep the point, drop the history.
+__global__ void k_reject(CotSolver *S)
+{
+    if (S->done || S->accepted) return;
+    if (S->mode == COT_SOLVE_REFERENCE) {
+        S->restart = 1;
+    } else if (S->k == 0) {
+        S->failed = 1;
+        S->done = 1;
+        return;
+    }
+    S->k = 0;
+    S->H0 = 1.0;
+    S->restarts++;
+    S->iter++;
+    if (S->iter >= S->max_iter) S->done = 1;
+}
+
+void launch_reject(CotSolver *S, cudaStream_t s) { k_reject<<<1, 1, 0, s>>>(S); }
+
+// The first evaluation becomes the current point without a line search.
+__global__ void k_init_from_eval(CotSolver *S, const CotEvalOut *out)
+{
+    S->last = *out;
+    S->evals++;
+}
+
+void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, cudaStream_t s)
+{
+    k_init_from_eval<<<1, 1, 0, s>>>(S, out);
+}
+
+}  // namespace cot

@@ -1,0 +1,175 @@
+/*
+ * causticot.h -- C ABI of the B200 semi-discrete optimal-transport solver.
+ *
+ * Replaces the first stage of the caustic pipeline: the `caustic_GPU`
+ * executable built from Optimal_Transport_rl/ in rmk523/caustic.  That
+ * executable is reached through a process + file contract
+ * (utils/basic_function.py:14-34 runs it; main.cu:51-342 reads the JSON and
+ * seed files and writes the weights and centroids).  These entry points are
+ * the in-process form of the same stages; each comment names the reference
+ * code it replaces.  The `caustic_GPU` shim in this package keeps the
+ * process + file contract on top of them.
+ *
+ * Conventions
+ *  - every function returns COT_OK (0) or a negative COT_E* code and never
+ *    aborts; cot_last_error() gives the message of the last failure;
+ *  - coordinates are doubles, sites interleaved xy[2*i], xy[2*i+1];
+ *  - domains are {xmin, xmax, ymin, ymax} (the reference's sample_domain /
+ *    proj_domain order, main.cu:81-83);
+ *  - the density image is density[ix + iy*nx] with nx pixels along x (the
+ *    reference's d_picture[i_x + i_y*size[0]], basic_function.cuh:805);
+ *  - pointer arguments are caller-owned and live in host memory unless
+ *    `mem` says COT_MEM_DEVICE (then they are device pointers on the
+ *    handle's device); the library owns its workspace;
+ *  - one handle per stream; a handle is not shared between host threads.
+ */
+#ifndef CAUSTICOT_H_
+#define CAUSTICOT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define COT_API __attribute__((visibility("default")))
+#else
+#define COT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COT_VERSION_MAJOR 0
+#define COT_VERSION_MINOR 1
+#define COT_VERSION_PATCH 0
+
+enum {
+    COT_OK = 0,
+    COT_EINVAL = -1,       /* bad argument */
+    COT_ECUDA = -2,        /* CUDA runtime error */
+    COT_ENOPROBLEM = -3,   /* cot_set_problem has not been called */
+    COT_ECAPACITY = -4,    /* caller buffer too small */
+    COT_ERING = -5,        /* a cell exceeded the vertex capacity */
+    COT_ENOTCONV = -6,     /* solver stopped before the tolerance */
+    COT_ETIMEOUT = -7,     /* a bounded device wait gave up */
+    COT_ENOMEM = -8        /* allocation failed */
+};
+
+enum { COT_MEM_HOST = 0, COT_MEM_DEVICE = 1 };
+
+/* Solver flavours.
+ * COT_SOLVE_REFERENCE: direct_ot's loop (ot_op.cuh:289-537): backtracking
+ *   with simple decrease from initial_step, reject when a ring is too
+ *   complex, restart at step <= 1e-4*initial_step, stop when the gradient
+ *   norm taken at the start of the iteration is below `tol` and no cell is
+ *   empty.
+ * COT_SOLVE_WOLFE: L-BFGS with a strong-Wolfe line search (bracket by
+ *   doubling, zoom by bisection), stop when max_i |mu_i - nu_i| / nu_i <= tol.
+ */
+enum { COT_SOLVE_REFERENCE = 0, COT_SOLVE_WOLFE = 1 };
+
+typedef struct cot_handle cot_handle;
+
+typedef struct {
+    int device;          /* CUDA device ordinal */
+    int bucket_size;     /* target sites per neighbour bucket (0: default 4) */
+    int warps_per_block; /* cell kernel launch shape (0: default) */
+    int max_ring;        /* ring-complexity reject threshold (0: 200, as
+                            ot_op.cuh:376 max_edge_num/2) */
+} cot_config;
+
+typedef struct {
+    int mode;            /* COT_SOLVE_* */
+    int history;         /* L-BFGS memory (reference: history_size) */
+    int max_iter;        /* reference: total_iter */
+    double tol;          /* see the mode */
+    double initial_step; /* reference: initial_step */
+    double c1, c2;       /* Wolfe constants (0: 1e-4, 0.9) */
+    int max_ls;          /* line-search trials per iteration (0: 30) */
+    int use_graph;       /* 1: run the iteration loop as a CUDA graph */
+} cot_solve_opts;
+
+typedef struct {
+    int iterations;
+    int evaluations;     /* objective evaluations incl. every trial */
+    int restarts;
+    int converged;
+    double f;            /* final objective */
+    double max_rel_err;  /* max_i |mu_i - nu_i| / nu_i at exit */
+    double grad_norm;    /* ||mu - nu||_2 at exit */
+    int empty_cells;     /* cells with mu_i == 0 at exit */
+    int ring_overflows;  /* trials rejected as too complex */
+    double ms;           /* device time of the solve */
+} cot_solve_stats;
+
+/* Library version. */
+COT_API int cot_version(int *major, int *minor, int *patch);
+
+/* Handle life cycle (replaces the cudaMalloc/cudaFree blocks of
+ * ot_op.cuh:121-152, 548-583). */
+COT_API int cot_create(const cot_config *cfg, cot_handle **out);
+COT_API int cot_destroy(cot_handle *h);
+
+/* Stream used by every call on the handle (NULL: the handle's own stream). */
+COT_API int cot_set_stream(cot_handle *h, void *cuda_stream);
+
+/* Problem definition: sites, target masses, target density, domain.
+ * Replaces main.cu:130-198 (reading proj_xy and the picture) plus the
+ * density normalisation of ot_op.cuh:81-88,154: the density is scaled so
+ * that it sums to sum(nu), which is the reference's area_scalar.
+ * Mirror sites (power_diagram.cpp:26-49) are not needed: a mirror never
+ * wins over its own site inside proj_domain, so every cell restricted to
+ * proj_domain is the same with or without them. */
+COT_API int cot_set_problem(cot_handle *h, const double *sites_xy, const double *nu, int n,
+                    const double *density, int nx, int ny, const double proj_domain[4],
+                    int mem);
+
+/* One objective + gradient evaluation at weights w (caller order).
+ * Replaces polygons_in_VD + compute_inte + compute_subtract + compute_f
+ * (ot_op.cuh:208-278, 364-403).  Outputs may be NULL.
+ *   f_total = sum_i f_i; mu[i]; g[i] = mu_i - nu_i; f_cell[i] = f_i. */
+COT_API int cot_eval(cot_handle *h, const double *w, double *f_total, double *mu, double *g,
+             double *f_cell, int mem);
+
+/* Cells at weights w, restricted to proj_domain: CCW rings and, for every
+ * ring edge, the index of the neighbouring site (-1..-4 for the domain
+ * sides bottom, right, top, left).  Replaces the polygons / start_num /
+ * length arrays of polygons_in_VD (power_diagram.cpp:8-134) after the
+ * domain clip of basic_function.cuh:763.  ring_offsets has n+1 entries;
+ * capacity is the size of ring_xy in vertices.  Host memory only. */
+COT_API int cot_cells(cot_handle *h, const double *w, int *ring_offsets, double *ring_xy,
+              int *ring_nbr, int capacity);
+
+/* Solve for the weights from w_inout (caller order).  Replaces the solver
+ * loop of direct_ot (ot_op.cuh:289-537). */
+COT_API int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts,
+              cot_solve_stats *stats, int mem);
+
+/* Density-weighted (weighted=1) or plain centroids of the cells at w and
+ * the exist flags.  Replaces compute_center (basic_function.cuh:1056-1191,
+ * ot_op.cuh:539-546). */
+COT_API int cot_centroids(cot_handle *h, const double *w, double *xy, unsigned char *exist,
+                  int weighted, int mem);
+
+/* Source masses of parallel light: areas of the unweighted cells of the
+ * source points inside sample_domain, normalised to total area_scalar.
+ * Replaces compute_clip_area + the normalisation of ot_op.cuh:90-92,158,
+ * 199-206.  Independent of the problem set on the handle. */
+COT_API int cot_source_masses(cot_handle *h, const double *points_xy, int n,
+                      const double sample_domain[4], double *nu_out);
+
+/* Diagnostic splat of nu over the pixels, nu_i * area(cell_i ∩ pixel) /
+ * area(cell_i) (render, basic_function.cuh:660-741), scaled by the
+ * reference's gray_multiple = sum(raw density) / area_scalar
+ * (ot_op.cuh:215).  out has nx*ny entries (host memory). */
+COT_API int cot_render(cot_handle *h, const double *w, double gray_multiple, double *out);
+
+/* Message of the last failure on this handle (or of the last failed
+ * cot_create when h is NULL). */
+COT_API int cot_last_error(cot_handle *h, char *buf, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAUSTICOT_H_ */
