@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SDOT solver on the plain large single instance.
+
+Workload: N = 65,536 sites (256x256 jittered grid, Gaussian-beam masses,
+sigma 0.35), 1024x1024 Gaussian-mixture target (K = 16, floor 1e-3), cold
+start w = 0, L-BFGS with memory 10 and a strong-Wolfe line search, stopped at
+max_i |mu_i - nu_i| / nu_i <= 1e-4.  One step = one complete solve.
+
+Metric: cell-evals/s = N x objective evaluations (every line-search trial
+counts) / solve time; the solve time itself is reported as solve_ms.
+
+  value  -- device-resident inputs, CUDA events on the launching stream
+  e2e    -- through the public API with host buffers: problem upload, the
+            solve, and the weights read back, every step
+  roofline -- the fused cell kernel: algorithmic bytes per evaluation
+            (8*H*W density + 48*N per-site) / its average launch time
+  cpu_baseline -- the CPU oracle (restated reference algorithm) on a bounded
+            sample of the same solve, on this machine's host cores
+
+With --gpus N (torchrun) every rank solves its own replica (the solver does
+not shard: replicas only), time = max over ranks.
+--impl reference times the CPU restatement of the reference's algorithm on
+this host (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "OT solve ms @1e-4 mass err: learned warm-start vs plain L-BFGS; cell-evals/s"
+UNIT = "cell-evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--tol", type=float, default=1e-4)
+    ap.add_argument("--history", type=int, default=10)
+    ap.add_argument("--cpu-sample-evals", type=int, default=6,
+                    help="oracle evaluations per CPU sample (about 1 s each at the default size)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(config):
+    from caustic_b200 import problems
+
+    p = problems.make(config)
+    return p, {"workload": f"sdot_config{config}_cold_lbfgs_wolfe", "n_sites": p.n, "image": list(p.size),
+               "target": "gaussian_mixture_floor1e-3", "masses": "beam_sigma0.35" if config in (2, 5) else "uniform",
+               "stop": "max_rel_mass_err<=1e-4", "lbfgs_memory": 10, "line_search": "strong_wolfe"}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the cell kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_cells_config2.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip().split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    c = [x.strip() for x in line.split(",")]
+                    if len(c) < 9:
+                        continue
+                    try:
+                        sm.append(float(c[1]))
+                        mx = float(c[2])
+                    except ValueError:
+                        continue
+                    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                    for nm, v in zip(names, c[5:9]):
+                        if v.lower() == "active":
+                            reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(p, evals, tol, history):
+    """Oracle (CPU restatement) on the first `evals` evaluations of the solve."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    prob = O.Problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+    t = time.perf_counter()
+    _, st = O.lbfgs_wolfe(prob, np.zeros(p.n), tol=tol, m=history, max_evals=evals)
+    dt = time.perf_counter() - t
+    return p.n * st.evaluations / dt, st.evaluations, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np  # noqa: F401
+
+    p, cfg = workload(args.config)
+    vals = []
+    tot_e = 0
+    tot_t = 0.0
+    for k in range(args.warmup + args.steps):
+        v, e, dt = cpu_baseline(p, args.cpu_sample_evals, args.tol, args.history)
+        if k >= args.warmup:
+            vals.append(v)
+            tot_e += e
+            tot_t += dt
+    value = p.n * tot_e / tot_t
+    cores = os.cpu_count()
+    sample = (f"first {args.cpu_sample_evals} objective evaluations of the cold-start L-BFGS per step, "
+              f"same problem; Qhull regular triangulation (1 thread) + C integration (OpenMP {cores} threads)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64, same generator as the GPU arm)", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's own solver needs CGAL 5.5/Eigen/Boost, absent here; this is the oracle port"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from caustic_b200 import capi
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    p, cfg = workload(args.config)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    solver = capi.Solver(device=local, profile=True)
+    solver.set_stream(stream.cuda_stream)
+    xy_d = torch.from_numpy(p.xy.reshape(-1)).to(dev)
+    nu_d = torch.from_numpy(p.nu).to(dev)
+    pic_d = torch.from_numpy(p.picture).to(dev)
+    solver.set_problem(xy_d, nu_d, pic_d, p.size, p.proj_domain)
+    w0 = torch.zeros(p.n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def solve():
+        return solver.solve(w0, mode=capi.SOLVE_WOLFE, history=args.history, max_iter=100000, tol=args.tol)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        w, st = solve()
+    torch.cuda.synchronize()
+    solver.kernel_stats(reset=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stats = []
+    with Clocks(local) as clk:
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(k & 255)  # evict L2 between solves
+            evs[k][0].record(stream)
+            w, st = solve()
+            evs[k][1].record(stream)
+            stats.append(st)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+    ks = solver.kernel_stats(reset=True)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    tot_ms = sum(step_ms)
+    evals = sum(s.evaluations for s in stats)
+    conv = all(s.converged for s in stats)
+    cell_evals = float(p.n) * evals
+    if dist is not None:
+        t = torch.tensor([tot_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+        c = torch.tensor([cell_evals], device=dev, dtype=torch.float64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        cell_evals = float(c.item())
+    value = cell_evals / (tot_ms * 1e-3)
+
+    # roofline of the fused cell kernel
+    hbm, peak_kind = peaks()
+    H, W = p.size[1], p.size[0]
+    alg_bytes = 8.0 * H * W + 48.0 * p.n
+    avg_ms = ks["cell_ms"] / max(ks["cell_launches"], 1)
+    achieved = alg_bytes / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
+    traffic = committed_traffic()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+            "kernel": "k_cells<64> (fused power cell + pixel integration)",
+            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms, "launches": ks["cell_launches"],
+            "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"}
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        xy_h = torch.from_numpy(p.xy.reshape(-1)).pin_memory()
+        nu_h = torch.from_numpy(p.nu).pin_memory()
+        pic_h = torch.from_numpy(p.picture).pin_memory()
+        w_h = torch.zeros(p.n, dtype=torch.float64).pin_memory()
+        s2 = capi.Solver(device=local)
+        s2.set_stream(stream.cuda_stream)
+        # warm the handle once
+        s2.set_problem(xy_h.numpy(), nu_h.numpy(), pic_h.numpy(), p.size, p.proj_domain)
+        s2.solve(w_h.numpy(), mode=capi.SOLVE_WOLFE, history=args.history, max_iter=100000, tol=args.tol)
+        torch.cuda.synchronize()
+        e_ev = 0
+        t_ms = 0.0
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s2.set_problem(xy_h.numpy(), nu_h.numpy(), pic_h.numpy(), p.size, p.proj_domain)
+            wout, st2 = s2.solve(w_h.numpy(), mode=capi.SOLVE_WOLFE, history=args.history, max_iter=100000,
+                                 tol=args.tol)
+            b.record(stream)
+            b.synchronize()
+            t_ms += a.elapsed_time(b)
+            e_ev += st2.evaluations
+        s2.close()
+        ce = float(p.n) * e_ev
+        if dist is not None:
+            t = torch.tensor([t_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_ms = float(t.item())
+            c = torch.tensor([ce], device=dev, dtype=torch.float64)
+            dist.all_reduce(c, op=dist.ReduceOp.SUM)
+            ce = float(c.item())
+        h2d = p.xy.nbytes + p.nu.nbytes + p.picture.nbytes + 8 * p.n
+        e2e = {"value": ce / (t_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(8 * p.n), "ms_per_step": t_ms / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, e, dt = cpu_baseline(p, args.cpu_sample_evals, args.tol, args.history)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"first {e} objective evaluations of the same cold-start solve ({dt:.1f} s)"}
+
+    if rank == 0:
+        cfg = dict(cfg)
+        cfg["parallelism"] = f"replicas{world}"
+        cfg["l2"] = "256 MiB buffer written between timed solves"
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded PCG64 jittered sites + Gaussian-mixture target)", "config": cfg,
+                "solve_ms": tot_ms / args.steps, "evaluations_per_solve": evals / args.steps,
+                "iterations_per_solve": sum(s.iterations for s in stats) / args.steps,
+                "max_rel_err": max(s.max_rel_err for s in stats), "converged": conv,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": ks["launches"]}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -13,7 +13,8 @@ from dataclasses import dataclass
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libcausticot.so")
+# CAUSTICOT_LIB selects another build of the same library (e.g. a measurement build)
+LIB_PATH = os.environ.get("CAUSTICOT_LIB") or os.path.join(_PKG, "libcausticot.so")
 
 COT_OK = 0
 COT_EINVAL = -1
@@ -33,13 +34,19 @@ SOLVE_WOLFE = 1
 
 EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
-    "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_last_error",
+    "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
+    "cot_last_error",
 ]
 
 
 class cot_config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("bucket_size", ctypes.c_int),
-                ("warps_per_block", ctypes.c_int), ("max_ring", ctypes.c_int)]
+                ("warps_per_block", ctypes.c_int), ("max_ring", ctypes.c_int), ("profile", ctypes.c_int)]
+
+
+class cot_kernel_stats(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_longlong), ("cell_launches", ctypes.c_longlong),
+                ("cell_ms", ctypes.c_double), ("evaluations", ctypes.c_longlong)]
 
 
 class cot_solve_opts(ctypes.Structure):
@@ -87,6 +94,7 @@ def load():
         L.cot_centroids.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
         L.cot_source_masses.argtypes = [vp, dp, ctypes.c_int, dp, dp]
         L.cot_render.argtypes = [vp, dp, ctypes.c_double, dp]
+        L.cot_get_kernel_stats.argtypes = [vp, ctypes.POINTER(cot_kernel_stats), ctypes.c_int]
         L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTED:
             getattr(L, name).restype = ctypes.c_int
@@ -134,10 +142,11 @@ class Solver:
     contiguous); outputs come back in the same kind as the input weights.
     """
 
-    def __init__(self, device: int = 0, bucket_size: int = 0, warps_per_block: int = 0, max_ring: int = 0):
+    def __init__(self, device: int = 0, bucket_size: int = 0, warps_per_block: int = 0, max_ring: int = 0,
+                 profile: bool = False):
         L = load()
         self._L = L
-        cfg = cot_config(device, bucket_size, warps_per_block, max_ring)
+        cfg = cot_config(device, bucket_size, warps_per_block, max_ring, int(bool(profile)))
         h = ctypes.c_void_p()
         rc = L.cot_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != COT_OK:
@@ -172,6 +181,13 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+    def kernel_stats(self, reset: bool = False) -> dict:
+        """Launch counts and summed cell-kernel device time (profile=True)."""
+        st = cot_kernel_stats()
+        self._check(self._L.cot_get_kernel_stats(self._h, ctypes.byref(st), int(bool(reset))))
+        return {"launches": st.launches, "cell_launches": st.cell_launches, "cell_ms": st.cell_ms,
+                "evaluations": st.evaluations}
 
     def set_stream(self, stream_ptr: int):
         self._check(self._L.cot_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

@@ -35,6 +35,7 @@ struct CotProblemDev {
     double *w = nullptr, *wt = nullptr, *d = nullptr, *mu = nullptr, *mut = nullptr, *fc = nullptr;
     double *phibar = nullptr;
     int *nv = nullptr, *ovf_list = nullptr, *ovf_count = nullptr;
+    int *nbc = nullptr, *nbn = nullptr;
     double *partials = nullptr;
     unsigned int *ticket = nullptr;
     CotEvalOut *out = nullptr;
@@ -55,6 +56,12 @@ struct cot_handle {
     CotProblemDev P;
     bool has_problem = false;
     CotSolver *hS = nullptr;  // pinned mirror of the control block
+    cot::CotCtx ctx;
+    cot::CotCtx &c()
+    {
+        ctx.s = stream;
+        return ctx;
+    }
 };
 
 static std::string g_create_err;
@@ -119,7 +126,7 @@ using namespace cot;
 static void free_problem(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
-                    P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_count, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
+                    P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_count, P.nbc, P.nbn, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
                     P.Yv};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -167,6 +174,18 @@ extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
     }
     configure_cells_kernels();
     h->stream = h->own_stream;
+    if (h->cfg.profile) {
+        const int cap = 1 << 16;
+        h->ctx.ev = new (std::nothrow) cudaEvent_t[cap];
+        if (h->ctx.ev) {
+            for (int k = 0; k < cap; k++) {
+                if (cudaEventCreate(&h->ctx.ev[k]) != cudaSuccess) break;
+                h->ctx.ev_cap = k + 1;
+            }
+            h->ctx.ev_cap &= ~1;
+        }
+        h->ctx.profile = true;
+    }
     *out = h;
     return COT_OK;
 }
@@ -177,6 +196,10 @@ extern "C" int cot_destroy(cot_handle *h)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_problem(h->P);
+    if (h->ctx.ev) {
+        for (int k = 0; k < h->ctx.ev_cap; k++) cudaEventDestroy(h->ctx.ev[k]);
+        delete[] h->ctx.ev;
+    }
     if (h->hS) cudaFreeHost(h->hS);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -187,6 +210,29 @@ extern "C" int cot_set_stream(cot_handle *h, void *s)
 {
     if (!h) return COT_EINVAL;
     h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return COT_OK;
+}
+
+extern "C" int cot_get_kernel_stats(cot_handle *h, cot_kernel_stats *out, int reset)
+{
+    if (!h || !out) return COT_EINVAL;
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    CotCtx &c = h->ctx;
+    double ms = 0.0;
+    for (int k = 0; k + 1 < c.ev_used; k += 2) {
+        float t = 0.0f;
+        COT_CUDA_TRY(cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]));
+        ms += t;
+    }
+    out->launches = c.launches;
+    out->cell_launches = c.cell_launches;
+    out->cell_ms = ms;
+    out->evaluations = c.evaluations;
+    if (reset) {
+        c.launches = c.cell_launches = c.evaluations = 0;
+        c.ev_used = 0;
+    }
     return COT_OK;
 }
 
@@ -354,7 +400,9 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
     if (e == cudaSuccess) e = A((void **)&P.nv, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.ovf_list, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.ovf_count, sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.ovf_count, 4 * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.nbc, N * COT_NBC * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.nbn, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.partials, (size_t)reduce_blocks(n) * (5 * COT_MAX_HIST + 8) * 8);
     if (e == cudaSuccess) e = A((void **)&P.ticket, sizeof(unsigned int));
     if (e == cudaSuccess) e = A((void **)&P.out, sizeof(CotEvalOut));
@@ -372,7 +420,8 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
-    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 4 * sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
 
     CotGeo &g = P.geo;
@@ -402,6 +451,8 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     for (int k = 0; k < 4; k++) g.pd[k] = pd[k];
     g.xs = xs;
     g.ys = ys;
+    g.ixs = 1.0 / xs;
+    g.iys = 1.0 / ys;
     g.margin = 1e-11 * L * L;
     return COT_OK;
 }
@@ -439,9 +490,11 @@ static int upload_sorted(cot_handle *h, const double *src, int mem, double *dst)
     size_t N = (size_t)P.n;
     if (mem == COT_MEM_DEVICE) {
         k_gather<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, src, dst);
+        h->ctx.launches++;
     } else {
         COT_CUDA_TRY(cudaMemcpyAsync(P.tmp, src, N * 8, cudaMemcpyHostToDevice, h->stream));
         k_gather<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, P.tmp, dst);
+        h->ctx.launches++;
     }
     COT_CUDA_TRY(cudaGetLastError());
     return COT_OK;
@@ -454,8 +507,10 @@ static int download_sorted(cot_handle *h, const double *src, double *dst, int me
     size_t N = (size_t)P.n;
     if (mem == COT_MEM_DEVICE) {
         k_scatter<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, src, dst);
+        h->ctx.launches++;
     } else {
         k_scatter<<<nblk(P.n), 256, 0, h->stream>>>(P.n, P.perm, src, P.tmp);
+        h->ctx.launches++;
         COT_CUDA_TRY(cudaMemcpyAsync(dst, P.tmp, N * 8, cudaMemcpyDeviceToHost, h->stream));
     }
     COT_CUDA_TRY(cudaGetLastError());
@@ -475,6 +530,9 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.nv = P.nv;
     a.ovf_list = P.ovf_list;
     a.ovf_count = P.ovf_count;
+    a.work = P.ovf_count + 1;
+    a.nbc = P.nbc;
+    a.nbn = P.nbn;
     return a;
 }
 
@@ -490,8 +548,8 @@ extern "C" int cot_eval(cot_handle *h, const double *w, double *f_total, double 
     int r;
     if ((r = upload_sorted(h, w, mem, P.w)) != COT_OK) return r;
     CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
-    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
-    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, s);
+    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
     COT_CUDA_TRY(cudaGetLastError());
     CotEvalOut o;
     COT_CUDA_TRY(cudaMemcpyAsync(&o, P.out, sizeof o, cudaMemcpyDeviceToHost, s));
@@ -534,7 +592,7 @@ extern "C" int cot_cells(cot_handle *h, const double *w, int *ring_offsets, doub
         a.ring_xy = rxy;
         a.ring_lab = rlab;
         a.ring_cap = cap;
-        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
         hxy.resize(N * cap * 2);
         hlab.resize(N * cap);
         e = cudaMemcpyAsync(hxy.data(), rxy, N * cap * 2 * 8, cudaMemcpyDeviceToHost, s);
@@ -596,7 +654,7 @@ extern "C" int cot_centroids(cot_handle *h, const double *w, double *xy, unsigne
     a.cen = cen;
     a.exist = ex;
     a.weighted = weighted ? 1 : 0;
-    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
     double *cen2 = cen + 2 * N;
     k_scatter2<<<nblk(P.n), 256, 0, s>>>(P.n, P.perm, cen, cen2);
     k_scatter_u8<<<nblk(P.n), 256, 0, s>>>(P.n, P.perm, ex, ex2);
@@ -628,7 +686,7 @@ extern "C" int cot_source_masses(cot_handle *h, const double *points_xy, int n, 
     cudaError_t e = cudaMemsetAsync(Q.w, 0, (size_t)n * 8, s);
     if (e == cudaSuccess) {
         CellsArgs a = cells_args(Q, Q.w, nullptr, nullptr);
-        launch_eval(Q.geo, a, h->cfg.warps_per_block, h->num_sms, s);
+        launch_eval(Q.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
         e = cudaMemcpyAsync(sorted.data(), Q.mut, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -713,33 +771,33 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
     // first point
     {
         CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
-        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
-        launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, s);
-        launch_init_from_eval(P.S, P.out, s);
-        launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, s);
+        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
+        launch_init_from_eval(P.S, P.out, h->c());
+        launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, h->c());
     }
     const size_t ctl = 16 * sizeof(int);
     int guard = 0;
     while (true) {
-        launch_begin_iteration(P.S, s);
-        launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, s);
+        launch_begin_iteration(P.S, h->c());
+        launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, h->c());
         COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
         COT_CUDA_TRY(cudaStreamSynchronize(s));
         if (hs.done) break;
         double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
         while (true) {
             CellsArgs a = cells_args(P, P.w, P.d, tptr);
-            launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, s);
-            launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, s);
+            launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+            launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, h->c());
             COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
             COT_CUDA_TRY(cudaStreamSynchronize(s));
             if (!hs.ls_active) break;
             if (++guard > 100000000) break;
         }
         if (hs.accepted)
-            launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, s);
+            launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, h->c());
         else
-            launch_reject(P.S, s);
+            launch_reject(P.S, h->c());
         COT_CUDA_TRY(cudaGetLastError());
     }
     COT_CUDA_TRY(cudaEventRecord(e1, s));

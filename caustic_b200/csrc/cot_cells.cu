@@ -23,11 +23,28 @@
 // covered pixels take a closed form.
 #include "cot_common.cuh"
 #include <math.h>
+#include <algorithm>
 
 namespace cot {
 
 #define FULLMASK 0xffffffffu
 #define COT_FRMAX 96
+
+#ifdef COT_PHASE_STATS
+// Measurement build only: per-phase cycle and event counters, kept per warp
+// in shared memory and added to the global totals once when the warp exits.
+__device__ unsigned long long cot_phase_stats[16];
+__shared__ unsigned long long cot_pst[8][16];
+#define PSTAT_ADD(k, v) do { if ((threadIdx.x & 31) == 0) cot_pst[threadIdx.x >> 5][k] += (unsigned long long)(v); } while (0)
+#define PSTAT_CLOCK(var) long long var = clock64()
+#define PSTAT_INIT() do { if ((threadIdx.x & 31) == 0) for (int q_ = 0; q_ < 16; q_++) cot_pst[threadIdx.x >> 5][q_] = 0; } while (0)
+#define PSTAT_FLUSH() do { if ((threadIdx.x & 31) == 0) for (int q_ = 0; q_ < 16; q_++) atomicAdd(&cot_phase_stats[q_], cot_pst[threadIdx.x >> 5][q_]); } while (0)
+#else
+#define PSTAT_INIT() do { } while (0)
+#define PSTAT_FLUSH() do { } while (0)
+#define PSTAT_ADD(k, v) do { } while (0)
+#define PSTAT_CLOCK(var) do { } while (0)
+#endif
 #define COT_WIN 1  // window radius in buckets
 
 // ---------------------------------------------------------------------------
@@ -229,11 +246,13 @@ __device__ __forceinline__ bool line_meet(double a1, double b1, double c1, doubl
     return true;
 }
 
+// Shared scratch of one warp for the large-ring path (rings up to MAXV).
 template <int MAXV>
 struct WarpPoly {
     double X[MAXV], Y[MAXV];          // vertices, relative to the site
     double A[MAXV], B[MAXV], C[MAXV]; // line of the edge leaving each vertex
     int L[MAXV];                      // its generator (site, or -1..-4)
+    double EIX[MAXV], EIY[MAXV], ESL[MAXV];  // per edge: 1/dx, 1/dy, dy/dx
     int fr[2][COT_FRMAX];             // tree traversal lists
     double elo[33], ehi[33];          // section of the cell at column lines
     double slo[32], shi[32];          // y-range of the cell in each column strip
@@ -312,9 +331,14 @@ __device__ int clip_poly(WarpPoly<MAXV> &P, int nv, double a, double b, double c
 // can never cut a later (smaller) one and is dropped for good.
 template <int MAXV>
 __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, double2 si, double wi,
-                          const double *__restrict__ wt, int lane, int &status)
+                          const double *__restrict__ wt, int lane, int &status, bool check_dup)
 {
     bool act = j >= 0;
+    if (act && check_dup) {
+        // a site whose line already bounds the polygon must not clip again
+        for (int k = 0; k < nv; k++)
+            if (P.L[k] == j) { act = false; break; }
+    }
     double a = 0.0, b = 0.0, c = 0.0, key = INFINITY;
     if (act) {
         double2 sj = g.xy[j];
@@ -332,7 +356,9 @@ __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, dou
             if (!cut) act = false;
         }
         unsigned mask = __ballot_sync(FULLMASK, cut);
+        PSTAT_ADD(4, 1);
         if (mask == 0u) break;
+        PSTAT_ADD(3, 1);
         double kk = cut ? key : INFINITY;
         int bl = lane;
 #pragma unroll
@@ -355,8 +381,8 @@ __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, dou
 }
 
 // Can no site of `node` beat site i anywhere on the current polygon?
-template <int MAXV>
-__device__ __forceinline__ bool node_excluded(const WarpPoly<MAXV> &P, int nv, const CotGeo &g, int node,
+template <class SP>
+__device__ __forceinline__ bool node_excluded(const SP &P, int nv, const CotGeo &g, int node,
                                               double2 si, double halfs2w)
 {
     double4 st = g.tstat[node];
@@ -402,8 +428,8 @@ __device__ __forceinline__ void vside_terms(double a, double b0, double b1, Mom 
 }
 
 // Section [lo, hi] of the polygon at the vertical line x (lo > hi: empty).
-template <int MAXV>
-__device__ __forceinline__ void section_at(const WarpPoly<MAXV> &P, int nv, double x, double &lo, double &hi)
+template <class SP>
+__device__ __forceinline__ void section_at(const SP &P, int nv, double x, double &lo, double &hi)
 {
     lo = INFINITY;
     hi = -INFINITY;
@@ -419,7 +445,7 @@ __device__ __forceinline__ void section_at(const WarpPoly<MAXV> &P, int nv, doub
         }
         double mn = fmin(px, qx), mx = fmax(px, qx);
         if (x < mn || x > mx) continue;
-        double yy = (x == px) ? py : (x == qx) ? qy : py + (x - px) * (qy - py) / (qx - px);
+        double yy = (x == px) ? py : (x == qx) ? qy : py + (x - px) * P.ESL[k];
         lo = fmin(lo, yy);
         hi = fmax(hi, yy);
     }
@@ -427,11 +453,42 @@ __device__ __forceinline__ void section_at(const WarpPoly<MAXV> &P, int nv, doub
 
 struct CellAcc { double mu, S, Mt, Mx, My; };
 
+// The part of the geometry the pixel integration needs, passed by value.
+struct PixGeo {
+    const double *rho;
+    double pd0, pd2, xs, ys, ixs, iys;
+    int nx, ny;
+};
+
+__device__ __forceinline__ PixGeo pix_geo(const CotGeo &g)
+{
+    PixGeo p;
+    p.rho = g.rho;
+    p.pd0 = g.pd[0];
+    p.pd2 = g.pd[2];
+    p.xs = g.xs;
+    p.ys = g.ys;
+    p.ixs = g.ixs;
+    p.iys = g.iys;
+    p.nx = g.nx;
+    p.ny = g.ny;
+    return p;
+}
+
 // Integrate the density over the cell (polygon relative to site si).
-template <int MAXV>
-__device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, double2 si, int lane)
+template <class SP>
+__device__ __noinline__ CellAcc integrate_cell(SP &P, int nv, const PixGeo g, double2 si, int lane)
 {
     CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // per-edge reciprocals and slopes: no divisions in the pixel loop
+    for (int k = lane; k < nv; k += 32) {
+        int kn = (k + 1 == nv) ? 0 : k + 1;
+        double dx = P.X[kn] - P.X[k], dy = P.Y[kn] - P.Y[k];
+        P.EIX[k] = dx != 0.0 ? 1.0 / dx : 0.0;
+        P.EIY[k] = dy != 0.0 ? 1.0 / dy : 0.0;
+        P.ESL[k] = dx != 0.0 ? dy / dx : 0.0;
+    }
+    __syncwarp();
     double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
     for (int k = lane; k < nv; k += 32) {
         mnx = fmin(mnx, P.X[k]); mxx = fmax(mxx, P.X[k]);
@@ -439,24 +496,29 @@ __device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, do
     }
     mnx = warp_min(mnx); mxx = warp_max(mxx); mny = warp_min(mny); mxy = warp_max(mxy);
     // pixel range of the bounding box (basic_function.cuh:791-799)
-    int lx = (int)floor((si.x + mnx - g.pd[0]) / g.xs);
-    int ly = (int)floor((si.y + mny - g.pd[2]) / g.ys);
-    int hx = (int)floor((si.x + mxx - g.pd[0]) / g.xs) + 1;
-    int hy = (int)floor((si.y + mxy - g.pd[2]) / g.ys) + 1;
+    // the reference's floor((min - d0) / step) .. floor((max - d0) / step) + 1
+    // (basic_function.cuh:791-794), widened by one pixel on each side so that
+    // the reciprocal's rounding can never drop a covered pixel; pixels outside
+    // the cell are skipped by the strip test below
+    int lx = (int)floor((si.x + mnx - g.pd0) * g.ixs) - 1;
+    int ly = (int)floor((si.y + mny - g.pd2) * g.iys) - 1;
+    int hx = (int)floor((si.x + mxx - g.pd0) * g.ixs) + 2;
+    int hy = (int)floor((si.y + mxy - g.pd2) * g.iys) + 2;
     lx = lx > 0 ? lx : 0;
     ly = ly > 0 ? ly : 0;
     hx = hx < g.nx ? hx : g.nx;
     hy = hy < g.ny ? hy : g.ny;
     if (hx <= lx || hy <= ly) return acc;
+    PSTAT_ADD(6, (hx - lx) * (hy - ly));
     const double pminx = mnx, pmaxx = mxx;
     double mu = 0.0, S = 0.0, Mt = 0.0, Mx = 0.0, My = 0.0;
     for (int cx0 = lx; cx0 < hx; cx0 += 32) {
         int cw = min(32, hx - cx0);
         // column lines cx0 .. cx0+cw
         for (int c = lane; c <= cw; c += 32) {
-            double xl = (double)(cx0 + c) * g.xs + g.pd[0] - si.x;
+            double xl = (double)(cx0 + c) * g.xs + g.pd0 - si.x;
             double lo, hi;
-            section_at<MAXV>(P, nv, xl, lo, hi);
+            section_at(P, nv, xl, lo, hi);
             P.elo[c] = lo;
             P.ehi[c] = hi;
             P.rv[c] = (pminx <= xl && xl < pmaxx) ? 1 : 0;  // right limit (left side of a pixel)
@@ -465,8 +527,8 @@ __device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, do
         __syncwarp();
         // y-range of the cell inside each column strip
         for (int c = lane; c < cw; c += 32) {
-            double xl = (double)(cx0 + c) * g.xs + g.pd[0] - si.x;
-            double xr = (double)(cx0 + c + 1) * g.xs + g.pd[0] - si.x;
+            double xl = (double)(cx0 + c) * g.xs + g.pd0 - si.x;
+            double xr = (double)(cx0 + c + 1) * g.xs + g.pd0 - si.x;
             double lo = INFINITY, hi = -INFINITY;
             if (P.rv[c]) { lo = fmin(lo, P.elo[c]); hi = fmax(hi, P.ehi[c]); }
             if (P.lv[c + 1]) { lo = fmin(lo, P.elo[c + 1]); hi = fmax(hi, P.ehi[c + 1]); }
@@ -484,10 +546,10 @@ __device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, do
             int c = p % cw, r = p / cw;
             int ix = cx0 + c, iy = ly + r;
             // pixel box exactly as basic_function.cuh:806-809, relative to the site
-            double x0 = (double)ix * g.xs + g.pd[0] - si.x;
-            double x1 = (double)(ix + 1) * g.xs + g.pd[0] - si.x;
-            double y0 = (double)iy * g.ys + g.pd[2] - si.y;
-            double y1 = (double)(iy + 1) * g.ys + g.pd[2] - si.y;
+            double x0 = (double)ix * g.xs + g.pd0 - si.x;
+            double x1 = (double)(ix + 1) * g.xs + g.pd0 - si.x;
+            double y0 = (double)iy * g.ys + g.pd2 - si.y;
+            double y1 = (double)(iy + 1) * g.ys + g.pd2 - si.y;
             if (!(P.shi[c] > y0 && P.slo[c] < y1)) continue;
             double xc = 0.5 * (x0 + x1), yc = 0.5 * (y0 + y1);
             double hxp = 0.5 * (x1 - x0), hyp = 0.5 * (y1 - y0);
@@ -503,22 +565,23 @@ __device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, do
                     double px = P.X[k], py = P.Y[k], qx = P.X[kn], qy = P.Y[kn];
                     if (px == qx && (px == x0 || px == x1)) continue;  // counted by the pixel side
                     if (fmax(px, qx) < x0 || fmin(px, qx) > x1 || fmax(py, qy) < y0 || fmin(py, qy) > y1) continue;
-                    // Liang-Barsky against the pixel box
+                    // Liang-Barsky against the pixel box (reciprocals precomputed)
                     double dx = qx - px, dy = qy - py, t0 = 0.0, t1 = 1.0;
-                    bool ok = true;
-                    double pp[4] = {-dx, dx, -dy, dy};
-                    double qq[4] = {px - x0, x1 - px, py - y0, y1 - py};
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        if (pp[e] == 0.0) {
-                            if (qq[e] < 0.0) ok = false;
-                        } else {
-                            double t = qq[e] / pp[e];
-                            if (pp[e] < 0.0) { if (t > t0) t0 = t; }
-                            else { if (t < t1) t1 = t; }
-                        }
+                    if (dx != 0.0) {
+                        double ta = (x0 - px) * P.EIX[k], tb = (x1 - px) * P.EIX[k];
+                        t0 = fmax(t0, fmin(ta, tb));
+                        t1 = fmin(t1, fmax(ta, tb));
+                    } else if (px < x0 || px > x1) {
+                        continue;
                     }
-                    if (!ok || !(t0 < t1)) continue;
+                    if (dy != 0.0) {
+                        double ta = (y0 - py) * P.EIY[k], tb = (y1 - py) * P.EIY[k];
+                        t0 = fmax(t0, fmin(ta, tb));
+                        t1 = fmin(t1, fmax(ta, tb));
+                    } else if (py < y0 || py > y1) {
+                        continue;
+                    }
+                    if (!(t0 < t1)) continue;
                     double ax0 = (t0 == 0.0 ? px : px + t0 * dx) - xc;
                     double by0 = (t0 == 0.0 ? py : py + t0 * dy) - yc;
                     double ax1 = (t1 == 1.0 ? qx : px + t1 * dx) - xc;
@@ -555,8 +618,8 @@ __device__ CellAcc integrate_cell(WarpPoly<MAXV> &P, int nv, const CotGeo &g, do
 }
 
 // Plain area centroid of the polygon (relative to the site).
-template <int MAXV>
-__device__ void poly_centroid(const WarpPoly<MAXV> &P, int nv, int lane, double &cx, double &cy)
+template <class SP>
+__device__ void poly_centroid(const SP &P, int nv, int lane, double &cx, double &cy)
 {
     double a = 0.0, mx = 0.0, my = 0.0;
     for (int k = lane; k < nv; k += 32) {
@@ -575,21 +638,472 @@ __device__ void poly_centroid(const WarpPoly<MAXV> &P, int nv, int lane, double 
 }
 
 // ---------------------------------------------------------------------------
-// the cell kernel
+// fast path: the polygon lives in registers, one vertex per lane
 // ---------------------------------------------------------------------------
-// mode 0: every cell (grid-stride); mode 1: the cells listed in ovf_list.
-template <int MAXV>
-__global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
+struct FastScratch {
+    double X[32], Y[32];              // polygon snapshot (tree tests, integration)
+    double A[32], B[32], C[32];       // compaction scratch of the general clip
+    int L[32];
+    double EIX[32], EIY[32], ESL[32]; // per edge: 1/dx, 1/dy, dy/dx
+    int fr[2][COT_FRMAX];
+    double elo[33], ehi[33];
+    double slo[32], shi[32];
+    unsigned char lv[33], rv[33];
+};
+
+// Lane k < nv holds vertex k and the line a x + b y <= c (generator l) of the
+// edge from vertex k to vertex k+1; coordinates relative to the site.
+struct RegPoly {
+    double x, y, a, b, c;
+    int l;
+    int nv;
+};
+
+__device__ __forceinline__ unsigned lanes_below(int n) { return n >= 32 ? FULLMASK : ((1u << n) - 1u); }
+
+// Clip by a x + b y <= c.  Returns false when the ring would exceed 32
+// vertices.  A convex ring crossed twice is a pure register permutation;
+// any other pattern (rounding on nearly collinear vertices) is compacted
+// through shared memory.
+__device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, int lab, int lane, FastScratch &S)
+{
+    const int nv = P.nv;
+    const bool valid = lane < nv;
+    const double d = side(a, b, c, P.x, P.y);
+    const unsigned vm = lanes_below(nv);
+    const unsigned outm = __ballot_sync(FULLMASK, valid && d > 0.0);
+    if (outm == 0u) return true;
+    if (outm == vm) {
+        P.nv = 0;
+        return true;
+    }
+    const int nx = (lane + 1 >= nv) ? 0 : lane + 1;
+    const double xn = __shfl_sync(FULLMASK, P.x, nx);
+    const double yn = __shfl_sync(FULLMASK, P.y, nx);
+    const double dn = __shfl_sync(FULLMASK, d, nx);
+    const bool in = !((outm >> lane) & 1u);
+    const bool inn = !((outm >> nx) & 1u);
+    const bool cross = valid && (in != inn);
+    double ix = 0.0, iy = 0.0;
+    if (cross) {
+        if (!line_meet(P.a, P.b, P.c, a, b, c, ix, iy)) {
+            double t = d / (d - dn);
+            ix = P.x + t * (xn - P.x);
+            iy = P.y + t * (yn - P.y);
+        }
+    }
+    const unsigned cm = __ballot_sync(FULLMASK, cross);
+    const int K = __popc(vm & ~outm);
+    if (__popc(cm) == 2) {
+        const unsigned em = __ballot_sync(FULLMASK, cross && !in);  // edge entering the half-plane
+        const int e = __ffs(em) - 1;
+        const int l = __ffs(cm & ~em) - 1;                         // edge leaving it
+        const int nn = K + 2;
+        if (nn > 32) return false;
+        // new ring: I_e, v_{e+1} .. v_{e+K} (= v_l), I_l
+        int src = e;
+        if (lane >= 1 && lane <= K) {
+            src = e + lane;
+            if (src >= nv) src -= nv;
+        } else if (lane == K + 1) {
+            src = l;
+        }
+        const double gx = __shfl_sync(FULLMASK, P.x, src);
+        const double gy = __shfl_sync(FULLMASK, P.y, src);
+        const double ga = __shfl_sync(FULLMASK, P.a, src);
+        const double gb = __shfl_sync(FULLMASK, P.b, src);
+        const double gc = __shfl_sync(FULLMASK, P.c, src);
+        const int gl = __shfl_sync(FULLMASK, P.l, src);
+        const double iex = __shfl_sync(FULLMASK, ix, e), iey = __shfl_sync(FULLMASK, iy, e);
+        const double ilx = __shfl_sync(FULLMASK, ix, l), ily = __shfl_sync(FULLMASK, iy, l);
+        if (lane == 0) {
+            P.x = iex; P.y = iey; P.a = ga; P.b = gb; P.c = gc; P.l = gl;
+        } else if (lane <= K) {
+            P.x = gx; P.y = gy; P.a = ga; P.b = gb; P.c = gc; P.l = gl;
+        } else if (lane == K + 1) {
+            P.x = ilx; P.y = ily; P.a = a; P.b = b; P.c = c; P.l = lab;
+        }
+        P.nv = nn;
+        return true;
+    }
+    const int cnt = valid ? ((in ? 1 : 0) + (cross ? 1 : 0)) : 0;
+    const int inc = warp_incl_scan(cnt, lane);
+    const int tot = __shfl_sync(FULLMASK, inc, 31);
+    if (tot > 32) return false;
+    __syncwarp();
+    if (valid) {
+        int p = inc - cnt;
+        if (in) {
+            S.X[p] = P.x; S.Y[p] = P.y; S.A[p] = P.a; S.B[p] = P.b; S.C[p] = P.c; S.L[p] = P.l;
+            p++;
+        }
+        if (cross) {
+            S.X[p] = ix; S.Y[p] = iy;
+            if (in) { S.A[p] = a; S.B[p] = b; S.C[p] = c; S.L[p] = lab; }
+            else { S.A[p] = P.a; S.B[p] = P.b; S.C[p] = P.c; S.L[p] = P.l; }
+        }
+    }
+    __syncwarp();
+    if (lane < tot) {
+        P.x = S.X[lane]; P.y = S.Y[lane]; P.a = S.A[lane]; P.b = S.B[lane]; P.c = S.C[lane]; P.l = S.L[lane];
+    }
+    __syncwarp();
+    P.nv = tot;
+    return true;
+}
+
+// Ascending bitonic sort of (key, idx) across the warp.
+__device__ __forceinline__ void warp_sort(double &key, int &idx, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            double ok = __shfl_xor_sync(FULLMASK, key, j);
+            int oi = __shfl_xor_sync(FULLMASK, idx, j);
+            bool up = (lane & k) == 0;
+            bool lower = (lane & j) == 0;
+            bool less = ok < key || (ok == key && oi < idx);
+            bool greater = ok > key || (ok == key && oi > idx);
+            if (lower == up ? less : greater) { key = ok; idx = oi; }
+        }
+    }
+}
+
+// Apply the candidates of one chunk (lane t holds site jl, -1 = none).  Each
+// lane first tests its own candidate against the whole ring (snapshot in
+// shared memory); only candidates that cut are then applied one by one with a
+// register clip (one that no longer cuts after an earlier clip is a no-op).
+// `nearest` applies the cutting ones in order of distance from the site.
+__device__ __noinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__restrict__ sxy, double2 si, double wi,
+                                            const double *__restrict__ wt, int lane, FastScratch &S, bool nearest)
+{
+    if (__ballot_sync(FULLMASK, jl >= 0) == 0u) return P;
+    double al = 0.0, bl = 0.0, cl = 0.0, key = INFINITY;
+    if (jl >= 0) {
+        double2 sj = sxy[jl];
+        al = sj.x - si.x;
+        bl = sj.y - si.y;
+        key = al * al + bl * bl;
+        cl = 0.5 * (key - (wt[jl] - wi));
+    }
+    const int nv = P.nv;
+    if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; S.L[lane] = P.l; }
+    __syncwarp();
+    bool cut = false;
+    if (jl >= 0) {
+        for (int k = 0; k < nv; k++) {
+            if (S.L[k] == jl) { cut = false; break; }   // already bounds the ring
+            if (side(al, bl, cl, S.X[k], S.Y[k]) > 0.0) cut = true;
+        }
+    }
+    __syncwarp();
+    unsigned have = __ballot_sync(FULLMASK, cut);
+#ifdef COT_PHASE_STATS
+    const int ntested = __popc(__ballot_sync(FULLMASK, jl >= 0));  // warp-wide, outside the lane-0 branch
+    PSTAT_ADD(4, ntested);
+#endif
+    if (have == 0u) return P;
+    int ord = lane;
+    if (nearest && __popc(have) > 1) {
+        double k2 = cut ? key : INFINITY;
+        warp_sort(k2, ord, lane);
+        have = lanes_below(__popc(have));
+    } else {
+        nearest = false;
+    }
+    while (have != 0u && P.nv > 0) {
+        const int t = __ffs(have) - 1;
+        have &= have - 1u;
+        const int src = nearest ? __shfl_sync(FULLMASK, ord, t) : t;
+        const int j = __shfl_sync(FULLMASK, jl, src);
+        const double a = __shfl_sync(FULLMASK, al, src);
+        const double b = __shfl_sync(FULLMASK, bl, src);
+        const double c = __shfl_sync(FULLMASK, cl, src);
+        const int before = P.nv;
+        if (!rclip(P, a, b, c, j, lane, S)) {
+            P.nv = -1;
+            return P;
+        }
+        if (P.nv != before) PSTAT_ADD(3, 1);
+    }
+    return P;
+}
+
+// Sites of `cnt[k]` consecutive ranges starting at `st[k]` (k = lane, up to
+// 32 ranges), applied in chunks of 32.  inc = inclusive scan of cnt.
+__device__ __noinline__ RegPoly apply_ranges(RegPoly P, int st, int cnt, int inc, int self, const double2 *__restrict__ sxy,
+                                             double2 si, double wi, const double *__restrict__ wt, int lane,
+                                             FastScratch &S, bool nearest)
+{
+    const int tot = __shfl_sync(FULLMASK, inc, 31);
+    for (int base = 0; base < tot && P.nv > 0; base += 32) {
+        const int t = base + lane;
+        // k = number of ranges that end at or before t
+        int k = 0;
+#pragma unroll
+        for (int sft = 16; sft >= 1; sft >>= 1) {
+            int v = __shfl_sync(FULLMASK, inc, k + sft - 1);
+            if (v <= t) k += sft;
+        }
+        const int ik = __shfl_sync(FULLMASK, inc, k & 31);
+        const int sk = __shfl_sync(FULLMASK, st, k & 31);
+        const int ck = __shfl_sync(FULLMASK, cnt, k & 31);
+        int j = (t < tot) ? sk + (t - (ik - ck)) : -1;
+        if (j == self) j = -1;
+        P = apply_chunk(P, j, sxy, si, wi, wt, lane, S, nearest);
+        if (P.nv < 0) return P;
+    }
+    return P;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int wpb = blockDim.x >> 5;
+    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[wib];
+    const double *__restrict__ wt = a.wt;
+    PSTAT_INIT();
+
+    while (true) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(a.work, 1);
+        idx = __shfl_sync(FULLMASK, idx, 0);
+        if (idx >= g.n) break;
+        const int i = idx;
+        const double2 si = g.xy[i];
+        const double wi = wt[i];
+        PSTAT_CLOCK(t0);
+        // domain rectangle, CCW, relative to the site
+        RegPoly P;
+        P.nv = 4;
+        {
+            const double x0 = g.pd[0] - si.x, x1 = g.pd[1] - si.x, y0 = g.pd[2] - si.y, y1 = g.pd[3] - si.y;
+            P.x = (lane == 1 || lane == 2) ? x1 : x0;
+            P.y = (lane >= 2) ? y1 : y0;
+            P.a = lane == 1 ? 1.0 : (lane == 3 ? -1.0 : 0.0);
+            P.b = lane == 0 ? -1.0 : (lane == 2 ? 1.0 : 0.0);
+            P.c = lane == 0 ? -y0 : (lane == 1 ? x1 : (lane == 2 ? y1 : -x0));
+            P.l = -(lane + 1);
+        }
+        bool ok = true;
+        const int bi = g.sbucket[i];
+        const int bu = bi % g.bx, bv = bi / g.bx;
+        // ---- 1. first candidates: last evaluation's neighbours, else the
+        //         3x3 buckets around the site, nearest first -------------------
+        const int ncache = (a.nbn != nullptr) ? a.nbn[i] : 0;
+        const bool cached = ncache > 0;
+        if (cached) {
+            int j = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
+            P = apply_chunk(P, j, g.xy, si, wi, wt, lane, S, false);
+        } else {
+            int bcnt = 0, bst = 0;
+            if (lane < 9) {
+                const int du = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
+                const int dv = (lane == 3 || lane == 5 || lane == 6) ? 1 : (lane == 4 || lane == 7 || lane == 8) ? -1 : 0;
+                const int u = bu + du, v = bv + dv;
+                if (u >= 0 && u < g.bx && v >= 0 && v < g.by) {
+                    const int b = u + v * g.bx;
+                    bst = g.bstart[b];
+                    bcnt = g.bstart[b + 1] - bst;
+                }
+            }
+            const int inc = warp_incl_scan(bcnt, lane);
+            P = apply_ranges(P, bst, bcnt, inc, i, g.xy, si, wi, wt, lane, S, true);
+        }
+        ok = P.nv >= 0;
+        const int win = cached ? -1 : COT_WIN;
+        PSTAT_CLOCK(t1);
+        PSTAT_ADD(0, t1 - t0);
+        PSTAT_ADD(10, cached ? 1 : 0);
+        // ---- 2. certificate over the bound tree --------------------------------
+        const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
+        bool brute = false;
+        if (ok && P.nv > 0 && g.nlev > 0) {
+            if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+            __syncwarp();
+            const int nv0 = P.nv;
+            const int top = g.nlev - 1;
+            int ncur = g.lev_w[top] * g.lev_h[top];
+            if (ncur > COT_FRMAX) brute = true;
+            int cur = 0;
+            if (!brute) {
+                // frontier entries are packed node coordinates u | v << 16
+                const int tw = g.lev_w[top];
+                for (int q = lane; q < ncur; q += 32) S.fr[0][q] = (q % tw) | ((q / tw) << 16);
+                __syncwarp();
+            }
+            for (int L = top; L >= 0 && !brute; L--) {
+                int nnext = 0;
+                const int off = g.lev_off[L], W = g.lev_w[L];
+                PSTAT_ADD(7, ncur);
+                for (int base = 0; base < ncur; base += 32) {
+                    const int q = (base + lane < ncur) ? S.fr[cur][base + lane] : -1;
+                    bool keep = false;
+                    int u = 0, v = 0;
+                    if (q >= 0) {
+                        u = q & 0xffff;
+                        v = q >> 16;
+                        const bool inwin = L == 0 && abs(u - bu) <= win && abs(v - bv) <= win;
+                        keep = !inwin && !node_excluded(S, nv0, g, off + u + v * W, si, halfs2w);
+                    }
+                    if (L == 0) {
+                        const unsigned m = __ballot_sync(FULLMASK, keep);
+                        const int cnt = __popc(m);
+                        if (nnext + cnt > COT_FRMAX) { brute = true; break; }
+                        if (keep) S.fr[1 - cur][nnext + __popc(m & ((1u << lane) - 1u))] = u + v * W;
+                        nnext += cnt;
+                    } else {
+                        const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1];
+                        int chc = 0;
+                        if (keep) {
+                            chc = (2 * u + 1 < cw ? 2 : 1) * (2 * v + 1 < ch ? 2 : 1);
+                        }
+                        const int inc = warp_incl_scan(chc, lane);
+                        const int cnt = __shfl_sync(FULLMASK, inc, 31);
+                        if (nnext + cnt > COT_FRMAX) { brute = true; break; }
+                        int pos = nnext + inc - chc;
+                        if (keep) {
+                            for (int bb = 0; bb < 2; bb++)
+                                for (int aa = 0; aa < 2; aa++)
+                                    if (2 * u + aa < cw && 2 * v + bb < ch) S.fr[1 - cur][pos++] = (2 * u + aa) | ((2 * v + bb) << 16);
+                        }
+                        nnext += cnt;
+                    }
+                }
+                __syncwarp();
+                if (brute) break;
+                cur = 1 - cur;
+                ncur = nnext;
+            }
+            if (!brute && ncur > 0) {
+                // sites of every surviving leaf, 32 leaves at a time
+                PSTAT_ADD(5, ncur);
+                for (int lb = 0; lb < ncur && ok && P.nv > 0; lb += 32) {
+                    int st = 0, cnt = 0;
+                    if (lb + lane < ncur) {
+                        const int b = S.fr[cur][lb + lane];
+                        st = g.bstart[b];
+                        cnt = g.bstart[b + 1] - st;
+                    }
+                    const int inc = warp_incl_scan(cnt, lane);
+                    P = apply_ranges(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
+                    ok = P.nv >= 0;
+                }
+            }
+        }
+        PSTAT_ADD(9, brute ? 1 : 0);
+        if (ok && brute && P.nv > 0) {
+            // frontier overflow: test every bucket against the current ring
+            const int nb = g.bx * g.by;
+            for (int base = 0; base < nb && ok && P.nv > 0; base += 32) {
+                if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+                __syncwarp();
+                const int b = base + lane;
+                bool keep = false;
+                if (b < nb) {
+                    const int u = b % g.bx, v = b / g.bx;
+                    const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
+                    keep = !inwin && !node_excluded(S, P.nv, g, b, si, halfs2w);
+                }
+                __syncwarp();
+                int st = 0, cnt = 0;
+                if (keep) {
+                    st = g.bstart[b];
+                    cnt = g.bstart[b + 1] - st;
+                }
+                const int inc = warp_incl_scan(cnt, lane);
+                P = apply_ranges(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
+                ok = P.nv >= 0;
+            }
+        }
+        if (!ok) {
+            // ring above 32 vertices: hand the cell to the large-capacity pass
+            if (lane == 0) {
+                const int slot = atomicAdd(a.ovf_count, 1);
+                a.ovf_list[slot] = i;
+                a.nv[i] = 33;
+            }
+            __syncwarp();
+            continue;
+        }
+        // ---- 3. integrate the density over the cell --------------------------
+        PSTAT_CLOCK(t2);
+        PSTAT_ADD(1, t2 - t1);
+        const int nv = P.nv;
+        if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+        __syncwarp();
+        CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (nv >= 3) acc = integrate_cell(S, nv, pix_geo(g), si, lane);
+        PSTAT_CLOCK(t3);
+        PSTAT_ADD(2, t3 - t2);
+        PSTAT_ADD(8, 1);
+        PSTAT_ADD(11, nv);
+        double pcx = 0.0, pcy = 0.0;
+        if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid(S, nv, lane, pcx, pcy);
+        if (a.ring_xy != nullptr && lane < nv && lane < a.ring_cap) {
+            a.ring_xy[2 * ((size_t)i * a.ring_cap + lane)] = si.x + P.x;
+            a.ring_xy[2 * ((size_t)i * a.ring_cap + lane) + 1] = si.y + P.y;
+            a.ring_lab[(size_t)i * a.ring_cap + lane] = P.l;
+        }
+        if (a.nbn != nullptr) {
+            // neighbours of this evaluation seed the next one
+            const bool isn = lane < nv && P.l >= 0;
+            const unsigned m = __ballot_sync(FULLMASK, isn);
+            const int pos = __popc(m & ((1u << lane) - 1u));
+            if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = P.l;
+            if (lane == 0) a.nbn[i] = min(__popc(m), COT_NBC);
+        }
+        if (lane == 0) {
+            a.mu[i] = acc.mu;
+            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941)
+            a.fc[i] = -wi * g.nu[i] - (acc.S - wi * acc.mu);
+            a.nv[i] = nv;
+            if (a.cen != nullptr) {
+                const bool ex = nv >= 3;
+                a.exist[i] = ex ? 1 : 0;
+                double cx = si.x, cy = si.y;
+                if (ex) {
+                    if (a.weighted && acc.Mt != 0.0) {
+                        cx = si.x + acc.Mx / acc.Mt;
+                        cy = si.y + acc.My / acc.Mt;
+                    } else {
+                        cx = si.x + pcx;
+                        cy = si.y + pcy;
+                    }
+                }
+                a.cen[2 * i] = cx;
+                a.cen[2 * i + 1] = cy;
+            }
+        }
+        __syncwarp();
+    }
+    PSTAT_FLUSH();
+}
+
+// ---------------------------------------------------------------------------
+// the cell kernel
+// ---------------------------------------------------------------------------
+// mode 0: every cell; mode 1: the cells listed in ovf_list.  Warps fetch
+// cells dynamically from a counter so that large cells do not leave a tail.
+template <int MAXV, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int mode)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
     WarpPoly<MAXV> &P = reinterpret_cast<WarpPoly<MAXV> *>(smem_raw)[wib];
     const double *__restrict__ wt = a.wt;
+    PSTAT_INIT();
 
-    int total = (mode == 0) ? g.n : *a.ovf_count;
-    for (int idx = blockIdx.x * wpb + wib; idx < total; idx += gridDim.x * wpb) {
+    const int total = (mode == 0) ? g.n : *a.ovf_count;
+    while (true) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(a.work + mode, 1);
+        idx = __shfl_sync(FULLMASK, idx, 0);
+        if (idx >= total) break;
         const int i = (mode == 0) ? idx : a.ovf_list[idx];
         const double2 si = g.xy[i];
         const double wi = wt[i];
@@ -604,16 +1118,23 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
             P.X[3] = x0; P.Y[3] = y1; P.A[3] = -1.0; P.B[3] = 0.0;  P.C[3] = -x0; P.L[3] = -4;
         }
         __syncwarp();
-        // ---- 1. neighbour window ------------------------------------------------
+        PSTAT_CLOCK(t0);
         const int bi = g.sbucket[i];
         const int bu = bi % g.bx, bv = bi / g.bx;
-        {
+        // ---- 1. first candidates: the cell's neighbours at the previous
+        //         evaluation, or the 3x3 buckets around the site ---------------
+        const int ncache = (a.nbn != nullptr) ? a.nbn[i] : 0;
+        const bool cached = ncache > 0;
+        if (cached) {
+            int j = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
+            nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status, false);
+        } else {
             int bcnt = 0, bst = 0;
             if (lane < 9) {
                 // own bucket, then the 4 edge neighbours, then the corners
-                const int tdu[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
-                const int tdv[9] = {0, 0, 0, 1, -1, 1, 1, -1, -1};
-                int u = bu + tdu[lane], v = bv + tdv[lane];
+                const int du = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
+                const int dv = (lane == 3 || lane == 5 || lane == 6) ? 1 : (lane == 4 || lane == 7 || lane == 8) ? -1 : 0;
+                int u = bu + du, v = bv + dv;
                 if (u >= 0 && u < g.bx && v >= 0 && v < g.by) {
                     int b = u + v * g.bx;
                     bst = g.bstart[b];
@@ -632,9 +1153,14 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
                     if (j < 0 && t < tot && t < ik) j = sk + (t - (ik - ck));
                 }
                 if (j == i) j = -1;
-                nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status);
+                nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status, false);
             }
         }
+        // leaves already processed in full (the window path only)
+        const int win = cached ? -1 : COT_WIN;
+        PSTAT_CLOCK(t1);
+        PSTAT_ADD(0, t1 - t0);
+        PSTAT_ADD(10, cached ? 1 : 0);
         // ---- 2. certificate over the bound tree --------------------------------
         const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
         bool brute = false;
@@ -650,16 +1176,17 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
             for (int L = top; L >= 0 && !brute && nv > 0 && status == 0; L--) {
                 int nnext = 0;
                 const int off = g.lev_off[L], W = g.lev_w[L];
+                PSTAT_ADD(7, ncur);
                 for (int base = 0; base < ncur; base += 32) {
                     int q = (base + lane < ncur) ? P.fr[cur][base + lane] : -1;
                     bool keep = false;
                     if (q >= 0) {
                         if (L == 0) {
                             int u = q % W, v = q / W;
-                            bool inwin = abs(u - bu) <= COT_WIN && abs(v - bv) <= COT_WIN;
-                            keep = !inwin && !node_excluded<MAXV>(P, nv, g, off + q, si, halfs2w);
+                            bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
+                            keep = !inwin && !node_excluded(P, nv, g, off + q, si, halfs2w);
                         } else {
-                            keep = !node_excluded<MAXV>(P, nv, g, off + q, si, halfs2w);
+                            keep = !node_excluded(P, nv, g, off + q, si, halfs2w);
                         }
                     }
                     if (L == 0) {
@@ -696,17 +1223,20 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
                 if (brute) break;
                 if (L == 0) {
                     // clip by the sites of every leaf that survived
+                    PSTAT_ADD(5, ncur);
                     for (int li = 0; li < ncur && nv > 0 && status == 0; li++) {
                         int b = P.fr[cur][li];
                         int s0 = g.bstart[b], s1 = g.bstart[b + 1];
                         for (int base = s0; base < s1 && nv > 0 && status == 0; base += 32) {
                             int j = base + lane < s1 ? base + lane : -1;
-                            nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status);
+                            if (j == i) j = -1;
+                            nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status, cached);
                         }
                     }
                 }
             }
         }
+        PSTAT_ADD(9, brute ? 1 : 0);
         if (brute && nv > 0 && status == 0) {
             // frontier overflow: test every bucket against the current polygon
             const int nb = g.bx * g.by;
@@ -715,8 +1245,8 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
                 bool keep = false;
                 if (b < nb) {
                     int u = b % g.bx, v = b / g.bx;
-                    bool inwin = abs(u - bu) <= COT_WIN && abs(v - bv) <= COT_WIN;
-                    keep = !inwin && !node_excluded<MAXV>(P, nv, g, b, si, halfs2w);
+                    bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
+                    keep = !inwin && !node_excluded(P, nv, g, b, si, halfs2w);
                 }
                 unsigned m = __ballot_sync(FULLMASK, keep);
                 while (m != 0u && nv > 0 && status == 0) {
@@ -726,7 +1256,8 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
                     int s0 = g.bstart[bb], s1 = g.bstart[bb + 1];
                     for (int sb = s0; sb < s1 && nv > 0 && status == 0; sb += 32) {
                         int j = sb + lane < s1 ? sb + lane : -1;
-                        nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status);
+                        if (j == i) j = -1;
+                        nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status, cached);
                     }
                 }
             }
@@ -746,16 +1277,32 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
             continue;
         }
         // ---- 3. integrate the density over the cell --------------------------
+        PSTAT_CLOCK(t2);
+        PSTAT_ADD(1, t2 - t1);
         CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (nv >= 3) acc = integrate_cell<MAXV>(P, nv, g, si, lane);
+        if (nv >= 3) acc = integrate_cell(P, nv, pix_geo(g), si, lane);
+        PSTAT_CLOCK(t3);
+        PSTAT_ADD(2, t3 - t2);
+        PSTAT_ADD(8, 1);
+        PSTAT_ADD(11, nv);
         double pcx = 0.0, pcy = 0.0;
-        if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid<MAXV>(P, nv, lane, pcx, pcy);
+        if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid(P, nv, lane, pcx, pcy);
         if (a.ring_xy != nullptr) {
             for (int k = lane; k < nv && k < a.ring_cap; k += 32) {
                 a.ring_xy[2 * ((size_t)i * a.ring_cap + k)] = si.x + P.X[k];
                 a.ring_xy[2 * ((size_t)i * a.ring_cap + k) + 1] = si.y + P.Y[k];
                 a.ring_lab[(size_t)i * a.ring_cap + k] = P.L[k];
             }
+        }
+        if (a.nbn != nullptr) {
+            // neighbours of this evaluation seed the next one
+            int lab = -1;
+            if (lane < nv) lab = P.L[lane];
+            bool isn = lab >= 0;
+            unsigned m = __ballot_sync(FULLMASK, isn);
+            int pos = __popc(m & ((1u << lane) - 1u));
+            if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = lab;
+            if (lane == 0) a.nbn[i] = min(__popc(m), COT_NBC);
         }
         if (lane == 0) {
             a.mu[i] = acc.mu;
@@ -781,40 +1328,77 @@ __global__ void __launch_bounds__(128) k_cells(CotGeo g, CellsArgs a, int mode)
         }
         __syncwarp();
     }
+    PSTAT_FLUSH();
 }
 
 static size_t cells_smem(int maxv, int warps)
 {
     switch (maxv) {
-    case 64: return sizeof(WarpPoly<64>) * (size_t)warps;
+    case 32: return sizeof(WarpPoly<32>) * (size_t)warps;
     default: return sizeof(WarpPoly<256>) * (size_t)warps;
     }
 }
 
-void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms, cudaStream_t s)
+#define CELLS_WPB 4
+#define CELLS_MINB 4
+static int g_cells_blocks_per_sm = 0;
+
+void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms, CotCtx &c)
 {
+    (void)warps_per_block;
+    cudaStream_t s = c.s;
     int nb = g.bx * g.by;
     k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar);
     k_bucket_bound<<<(nb + 127) / 128, 128, 0, s>>>(g, a.wt, a.phibar);
+    c.launches += 2;
     for (int L = 1; L < g.nlev; L++) {
         int cnt = g.lev_w[L] * g.lev_h[L];
         k_tree_level<<<(cnt + 127) / 128, 128, 0, s>>>(g, L);
+        c.launches++;
     }
-    cudaMemsetAsync(a.ovf_count, 0, sizeof(int), s);
-    int wpb = warps_per_block > 0 ? warps_per_block : 4;
-    int blocks = (g.n + wpb - 1) / wpb;
-    size_t sm = cells_smem(64, wpb);
-    k_cells<64><<<blocks, 32 * wpb, sm, s>>>(g, a, 0);
-    // overflowing cells (rare): one warp per block, 256-vertex rings
-    int ob = num_sms > 0 ? num_sms : 148;
-    k_cells<256><<<ob, 32, cells_smem(256, 1), s>>>(g, a, 1);
+    // ovf_count and the two work counters are contiguous
+    cudaMemsetAsync(a.ovf_count, 0, 3 * sizeof(int), s);
+    int sms = num_sms > 0 ? num_sms : 148;
+    int per_sm = g_cells_blocks_per_sm > 0 ? g_cells_blocks_per_sm : CELLS_MINB;
+    int want = (g.n + CELLS_WPB - 1) / CELLS_WPB;
+    int blocks = std::min(want, sms * per_sm);
+    size_t sm = sizeof(FastScratch) * CELLS_WPB;
+    bool timed = c.profile && c.ev != nullptr && c.ev_used + 2 <= c.ev_cap;
+    if (timed) cudaEventRecord(c.ev[c.ev_used], s);
+    k_cells_fast<CELLS_MINB><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a);
+    if (timed) {
+        cudaEventRecord(c.ev[c.ev_used + 1], s);
+        c.ev_used += 2;
+    }
+    // cells above 32 vertices (rare): one warp per block, 256-vertex rings
+    k_cells<256, 1><<<sms, 32, cells_smem(256, 1), s>>>(g, a, 1);
+    c.launches += 2;
+    c.cell_launches += 1;
+    c.evaluations += 1;
 }
 
-// Dynamic shared memory above 48 KB needs an opt-in per kernel.
+#ifdef COT_PHASE_STATS
+extern "C" __attribute__((visibility("default"))) int cot_debug_phase_stats(unsigned long long *out, int reset)
+{
+    cudaDeviceSynchronize();
+    cudaMemcpyFromSymbol(out, cot_phase_stats, sizeof(unsigned long long) * 16);
+    if (reset) {
+        unsigned long long z[16] = {0};
+        cudaMemcpyToSymbol(cot_phase_stats, z, sizeof z);
+    }
+    return 0;
+}
+#endif
+
 void configure_cells_kernels()
 {
-    cudaFuncSetAttribute(k_cells<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(64, 8));
-    cudaFuncSetAttribute(k_cells<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(256, 1));
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(FastScratch) * CELLS_WPB));
+    cudaFuncSetAttribute(k_cells<256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(256, 1));
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB>, 32 * CELLS_WPB,
+                                                      sizeof(FastScratch) * CELLS_WPB) == cudaSuccess && nb > 0)
+        g_cells_blocks_per_sm = nb;
 }
 
 }  // namespace cot

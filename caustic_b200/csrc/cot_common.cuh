@@ -19,6 +19,7 @@
 #define COT_MAX_LEVELS 24
 #define COT_MAX_HIST 32
 #define COT_BASIS (2 * COT_MAX_HIST + 1)
+#define COT_NBC 16  // cached neighbours per cell
 
 // Static geometry, passed by value to the kernels.
 struct CotGeo {
@@ -40,6 +41,7 @@ struct CotGeo {
     int nx, ny;            // pixels along x, along y
     double pd[4];          // proj_domain {xmin, xmax, ymin, ymax}
     double xs, ys;         // pixel extent (reference x_step, y_step)
+    double ixs, iys;       // their reciprocals
     double margin;         // safety margin of the plane-bound exclusion test
 };
 
@@ -103,6 +105,18 @@ struct CotSolver {
 
 namespace cot {
 
+// Launch context: the stream plus the kernel accounting of the handle.
+struct CotCtx {
+    cudaStream_t s = nullptr;
+    long long launches = 0;
+    long long cell_launches = 0;
+    long long evaluations = 0;
+    bool profile = false;
+    cudaEvent_t *ev = nullptr;  // pool of event pairs (profile)
+    int ev_cap = 0;
+    int ev_used = 0;
+};
+
 // Launchers implemented in cot_cells.cu.
 struct CellsArgs {
     const double *w;       // weights (base point)
@@ -114,7 +128,10 @@ struct CellsArgs {
     double *fc;            // per cell objective out
     int *nv;               // per cell ring size out
     int *ovf_list;         // cells to redo with the large ring capacity
-    int *ovf_count;        // device counter
+    int *ovf_count;        // device counters: [0] overflow count, [1..2] work
+    int *work;             // = ovf_count + 1
+    int *nbc;              // cached neighbours, COT_NBC per cell (nullable)
+    int *nbn;              // their count per cell (0: none)
     double *cen;           // centroids (nullable)
     unsigned char *exist;  // exist flags (nullable)
     int weighted;          // centroid flavour
@@ -124,21 +141,21 @@ struct CellsArgs {
 };
 
 void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms,
-                 cudaStream_t s);
+                 CotCtx &c);
 void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const int *nv,
                    const double *wt, const double *d, int max_ring, double *partials,
-                   unsigned int *ticket, CotEvalOut *out, CotSolver *solver, cudaStream_t s);
+                   unsigned int *ticket, CotEvalOut *out, CotSolver *solver, CotCtx &c);
 int reduce_blocks(int n);
 
 // Launchers implemented in cot_solver.cu.
-void launch_begin_iteration(CotSolver *S, cudaStream_t s);
+void launch_begin_iteration(CotSolver *S, CotCtx &c);
 void launch_direction(const CotGeo &g, const CotSolver *S, const double *Sv, const double *Yv,
-                      const double *mu, double *d, cudaStream_t s);
+                      const double *mu, double *d, CotCtx &c);
 void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double *w,
                    const double *wt, double *mu, const double *mut, const double *d,
-                   double *partials, unsigned int *ticket, int initial, cudaStream_t s);
-void launch_reject(CotSolver *S, cudaStream_t s);
-void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, cudaStream_t s);
+                   double *partials, unsigned int *ticket, int initial, CotCtx &c);
+void launch_reject(CotSolver *S, CotCtx &c);
+void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c);
 void configure_cells_kernels();
 
 }  // namespace cot

@@ -189,11 +189,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_eval(int n, const double
 
 void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const int *nv, const double *wt,
                    const double *d, int max_ring, double *partials, unsigned int *ticket, CotEvalOut *out,
-                   CotSolver *solver, cudaStream_t s)
+                   CotSolver *solver, CotCtx &c)
 {
     (void)wt;
     int nb = reduce_blocks(g.n);
-    k_reduce_eval<<<nb, RED_THREADS, 0, s>>>(g.n, mu, fc, nv, g.nu, d, max_ring, partials, ticket, out, solver);
+    k_reduce_eval<<<nb, RED_THREADS, 0, c.s>>>(g.n, mu, fc, nv, g.nu, d, max_ring, partials, ticket, out, solver);
+    c.launches++;
 }
 
 // ---------------------------------------------------------------------------
@@ -254,7 +255,11 @@ __global__ void k_begin_iteration(CotSolver *S)
     S->final_eval = 0;
 }
 
-void launch_begin_iteration(CotSolver *S, cudaStream_t s) { k_begin_iteration<<<1, 32, 0, s>>>(S); }
+void launch_begin_iteration(CotSolver *S, CotCtx &c)
+{
+    k_begin_iteration<<<1, 32, 0, c.s>>>(S);
+    c.launches++;
+}
 
 // d = sum_j delta_j basis_j
 __global__ void k_direction(int n, const CotSolver *__restrict__ S, const double *__restrict__ Sv,
@@ -278,11 +283,12 @@ __global__ void k_direction(int n, const CotSolver *__restrict__ S, const double
 }
 
 void launch_direction(const CotGeo &g, const CotSolver *S, const double *Sv, const double *Yv, const double *mu,
-                      double *d, cudaStream_t s)
+                      double *d, CotCtx &c)
 {
     int blocks = (g.n + 255) / 256;
     if (blocks > 4 * 148) blocks = 4 * 148;
-    k_direction<<<blocks, 256, 0, s>>>(g.n, S, Sv, Yv, mu, g.nu, d);
+    k_direction<<<blocks, 256, 0, c.s>>>(g.n, S, Sv, Yv, mu, g.nu, d);
+    c.launches++;
 }
 
 // Accept the trial: s_h = t d, y_h = mu_t - mu, w = w_t, mu = mu_t, then the
@@ -417,10 +423,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
 
 void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double *w, const double *wt, double *mu,
                    const double *mut, const double *d, double *partials, unsigned int *ticket, int initial,
-                   cudaStream_t s)
+                   CotCtx &c)
 {
     int nb = reduce_blocks(g.n);
-    k_accept<<<nb, RED_THREADS, 0, s>>>(g.n, S, Sv, Yv, w, wt, mu, mut, g.nu, d, partials, ticket, initial);
+    k_accept<<<nb, RED_THREADS, 0, c.s>>>(g.n, S, Sv, Yv, w, wt, mu, mut, g.nu, d, partials, ticket, initial);
+    c.launches++;
 }
 
 // Line search gave up (ot_op.cuh:413-425): keep the point, drop the history.
@@ -441,7 +448,11 @@ __global__ void k_reject(CotSolver *S)
     if (S->iter >= S->max_iter) S->done = 1;
 }
 
-void launch_reject(CotSolver *S, cudaStream_t s) { k_reject<<<1, 1, 0, s>>>(S); }
+void launch_reject(CotSolver *S, CotCtx &c)
+{
+    k_reject<<<1, 1, 0, c.s>>>(S);
+    c.launches++;
+}
 
 // The first evaluation becomes the current point without a line search.
 __global__ void k_init_from_eval(CotSolver *S, const CotEvalOut *out)
@@ -450,9 +461,10 @@ __global__ void k_init_from_eval(CotSolver *S, const CotEvalOut *out)
     S->evals++;
 }
 
-void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, cudaStream_t s)
+void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c)
 {
-    k_init_from_eval<<<1, 1, 0, s>>>(S, out);
+    k_init_from_eval<<<1, 1, 0, c.s>>>(S, out);
+    c.launches++;
 }
 
 }  // namespace cot

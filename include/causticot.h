@@ -76,7 +76,17 @@ typedef struct {
     int warps_per_block; /* cell kernel launch shape (0: default) */
     int max_ring;        /* ring-complexity reject threshold (0: 200, as
                             ot_op.cuh:376 max_edge_num/2) */
+    int profile;         /* 1: time every cell-kernel launch with CUDA events
+                            recorded on the launching stream */
 } cot_config;
+
+/* Kernel accounting of a handle (no reference counterpart: measurement). */
+typedef struct {
+    long long launches;       /* kernels this library launched */
+    long long cell_launches;  /* launches of the fused cell kernel */
+    double cell_ms;           /* their summed device time (profile=1) */
+    long long evaluations;    /* objective evaluations */
+} cot_kernel_stats;
 
 typedef struct {
     int mode;            /* COT_SOLVE_* */
@@ -163,6 +173,10 @@ COT_API int cot_source_masses(cot_handle *h, const double *points_xy, int n,
  * reference's gray_multiple = sum(raw density) / area_scalar
  * (ot_op.cuh:215).  out has nx*ny entries (host memory). */
 COT_API int cot_render(cot_handle *h, const double *w, double gray_multiple, double *out);
+
+/* Kernel accounting since the last reset; waits for the handle's stream.
+ * reset=1 clears the counters after reading. */
+COT_API int cot_get_kernel_stats(cot_handle *h, cot_kernel_stats *out, int reset);
 
 /* Message of the last failure on this handle (or of the last failed
  * cot_create when h is NULL). */

@@ -438,7 +438,7 @@ def max_rel_error(mu, nu):
 
 
 def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0.9,
-                max_ls=30, max_ring=None):
+                max_ls=30, max_ring=None, max_evals=None):
     """L-BFGS with a strong-Wolfe line search and the max-relative mass stop.
 
     Same rules as the device solver (caustic_b200 csrc/cot_solver.cu):
@@ -463,6 +463,8 @@ def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0
         st.history.append((f, err))
         if err <= tol:
             st.converged = True
+            break
+        if max_evals is not None and st.evaluations >= max_evals:
             break
         q = -g
         cnt = min(k, m)
@@ -489,6 +491,8 @@ def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0
         e_lo = None
         acc = None
         for _ in range(max_ls):
+            if max_evals is not None and st.evaluations >= max_evals:
+                break
             wt = w + t * d
             e = evaluate(prob, wt)
             st.evaluations += 1
