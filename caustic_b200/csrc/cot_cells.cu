@@ -238,11 +238,14 @@ __device__ __forceinline__ bool line_meet(double a1, double b1, double c1, doubl
         x = (c1 - b1 * y) / a1;
         return true;
     }
-    double det = a1 * b2 - a2 * b1;
+    // uncontracted products: swapping the two lines negates numerator and
+    // denominator exactly, so a vertex does not depend on which line clipped
+    // which
+    double det = __dsub_rn(__dmul_rn(a1, b2), __dmul_rn(a2, b1));
     double sc = (fabs(a1) + fabs(b1)) * (fabs(a2) + fabs(b2));
     if (!(fabs(det) > 1e-13 * sc)) return false;
-    x = (c1 * b2 - c2 * b1) / det;
-    y = (a1 * c2 - a2 * c1) / det;
+    x = __ddiv_rn(__dsub_rn(__dmul_rn(c1, b2), __dmul_rn(c2, b1)), det);
+    y = __ddiv_rn(__dsub_rn(__dmul_rn(a1, c2), __dmul_rn(a2, c1)), det);
     return true;
 }
 
@@ -1033,6 +1036,21 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
         PSTAT_CLOCK(t2);
         PSTAT_ADD(1, t2 - t1);
         const int nv = P.nv;
+        if (nv >= 3) {
+            // canonical ring start (smallest edge generator) so the integration
+            // sums in the same order whatever order the clips came in
+            const int key = lane < nv ? P.l : 0x7fffffff;
+            const int mn = __reduce_min_sync(FULLMASK, key);
+            const int r = __ffs(__ballot_sync(FULLMASK, key == mn)) - 1;
+            int src = lane + r;
+            if (src >= nv) src -= nv;
+            P.x = __shfl_sync(FULLMASK, P.x, src);
+            P.y = __shfl_sync(FULLMASK, P.y, src);
+            P.a = __shfl_sync(FULLMASK, P.a, src);
+            P.b = __shfl_sync(FULLMASK, P.b, src);
+            P.c = __shfl_sync(FULLMASK, P.c, src);
+            P.l = __shfl_sync(FULLMASK, P.l, src);
+        }
         if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
         __syncwarp();
         CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};

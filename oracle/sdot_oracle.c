@@ -338,20 +338,25 @@ ORC_API void orc_render(int n, const double *ring, const int *start, const int *
 
 typedef struct { double a, b, c; } orc_line; /* a x + b y <= c */
 
+/* Half-plane of generator j for cell i in coordinates translated to s_i
+ * (x' = x - s_i), the way CGAL's weighted-circumcentre constructions work on
+ * differences to one of the points:  2 e.x' <= |e|^2 - (w_j - w_i),
+ * e = s_j - s_i.  Box sides use the translated box. */
 static orc_line orc_gen_line(int i, int j, const double *xy, const double *w, const double *box)
 {
     orc_line L;
+    double xi = xy[2 * i], yi = xy[2 * i + 1];
     if (j >= 0) {
-        double xi = xy[2 * i], yi = xy[2 * i + 1], xj = xy[2 * j], yj = xy[2 * j + 1];
-        L.a = 2.0 * (xj - xi);
-        L.b = 2.0 * (yj - yi);
-        L.c = (xj * xj + yj * yj - w[j]) - (xi * xi + yi * yi - w[i]);
+        double ex = xy[2 * j] - xi, ey = xy[2 * j + 1] - yi;
+        L.a = 2.0 * ex;
+        L.b = 2.0 * ey;
+        L.c = (ex * ex + ey * ey) - (w[j] - w[i]);
     } else {
         switch (j) {
-        case -1: L.a = 0; L.b = -1; L.c = -box[2]; break; /* y >= ymin */
-        case -2: L.a = 1; L.b = 0; L.c = box[1]; break;   /* x <= xmax */
-        case -3: L.a = 0; L.b = 1; L.c = box[3]; break;   /* y <= ymax */
-        default: L.a = -1; L.b = 0; L.c = -box[0]; break; /* x >= xmin */
+        case -1: L.a = 0; L.b = -1; L.c = -(box[2] - yi); break; /* y >= ymin */
+        case -2: L.a = 1; L.b = 0; L.c = box[1] - xi; break;     /* x <= xmax */
+        case -3: L.a = 0; L.b = 1; L.c = box[3] - yi; break;     /* y <= ymax */
+        default: L.a = -1; L.b = 0; L.c = -(box[0] - xi); break; /* x >= xmin */
         }
     }
     return L;
@@ -374,10 +379,11 @@ static int orc_one_cell(int i, const int *nbr, int nn, const double *xy, const d
     int lab[2][ORC_MAXD / 2];
     int cur = 0, nv = 4;
     int vcap = ORC_MAXD / 2;
-    px[0][0] = box[0]; py[0][0] = box[2]; lab[0][0] = -1;
-    px[0][1] = box[1]; py[0][1] = box[2]; lab[0][1] = -2;
-    px[0][2] = box[1]; py[0][2] = box[3]; lab[0][2] = -3;
-    px[0][3] = box[0]; py[0][3] = box[3]; lab[0][3] = -4;
+    const double xi = xy[2 * i], yi = xy[2 * i + 1];
+    px[0][0] = box[0] - xi; py[0][0] = box[2] - yi; lab[0][0] = -1;
+    px[0][1] = box[1] - xi; py[0][1] = box[2] - yi; lab[0][1] = -2;
+    px[0][2] = box[1] - xi; py[0][2] = box[3] - yi; lab[0][2] = -3;
+    px[0][3] = box[0] - xi; py[0][3] = box[3] - yi; lab[0][3] = -4;
     for (int k = 0; k < nn && nv > 0; k++) {
         int j = nbr[k];
         if (j == i) continue;
@@ -427,8 +433,8 @@ static int orc_one_cell(int i, const int *nbr, int nn, const double *xy, const d
             double yy = (A.a * B.c - A.c * B.a) / det;
             if (isfinite(xx) && isfinite(yy)) { x = xx; y = yy; }
         }
-        out_xy[2 * v] = x;
-        out_xy[2 * v + 1] = y;
+        out_xy[2 * v] = xi + x;
+        out_xy[2 * v + 1] = yi + y;
         out_lab[v] = lab[cur][v];
     }
     return nv;

@@ -1,0 +1,263 @@
+"""GPU path (libcausticot.so through the C ABI) against the CPU oracle.
+
+Tolerances: cell masses and gradients agree to 1e-10 relative to the largest
+mass; the objective to 1e-9 relative (it is a sum of terms of both signs);
+adjacency bit-exact for every shared edge longer than 1e-9 of the site pitch.
+"""
+import gzip
+import json
+import os
+
+import numpy as np
+import pytest
+
+from caustic_b200 import capi, problems, seeds
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+MU_TOL = 1e-10
+F_TOL = 1e-9
+
+
+def oracle_problem(p):
+    return O.Problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+
+
+def solver_for(p, **kw):
+    s = capi.Solver(**kw)
+    s.set_problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+    return s
+
+
+def gpu_adjacency(s, w, min_len):
+    off, xy, nb = s.cells(w)
+    out = set()
+    for i in range(len(off) - 1):
+        R = xy[off[i]:off[i + 1]]
+        L = nb[off[i]:off[i + 1]]
+        if len(R) == 0:
+            continue
+        Q = np.roll(R, -1, axis=0)
+        ln = np.hypot(*(Q - R).T)
+        for k in range(len(L)):
+            if L[k] >= 0 and ln[k] > min_len:
+                out.add((min(i, int(L[k])), max(i, int(L[k]))))
+    return out, off
+
+
+def check_eval(p, w, s=None):
+    prob = oracle_problem(p)
+    s = s or solver_for(p)
+    f, mu, g, fc = s.eval(w)
+    ev = O.evaluate(prob, w, keep_cells=True)
+    scale = np.abs(ev.mu).max()
+    assert np.abs(mu - ev.mu).max() <= MU_TOL * scale
+    assert np.abs(g - ev.g).max() <= MU_TOL * scale
+    assert abs(f - ev.f) <= F_TOL * max(abs(ev.f), np.abs(ev.fcell).sum())
+    pitch = 1.0 / np.sqrt(p.n)
+    ga, _ = gpu_adjacency(s, w, 1e-9 * pitch)
+    oa = O.adjacency(ev.cells, 1e-9 * pitch)
+    assert ga == oa
+    return s, ev
+
+
+@pytest.mark.parametrize("g,res,beam", [(8, 32, False), (24, 96, False), (32, 128, True)])
+def test_eval_parity_small(gpu, g, res, beam):
+    p = problems.make(1, g=g, res=res, beam=beam)
+    s = solver_for(p)
+    rng = np.random.default_rng(g)
+    check_eval(p, np.zeros(p.n), s)
+    check_eval(p, rng.normal(0, 0.3 / p.n, p.n), s)
+    check_eval(p, rng.normal(0, 1.0 / p.n, p.n), s)   # strongly weighted: hidden cells appear
+
+
+def test_eval_parity_config1_full(gpu):
+    """N=4096, 256x256 mixture: masses, gradient, objective, adjacency."""
+    p = problems.make(1)
+    s = solver_for(p)
+    check_eval(p, np.zeros(p.n), s)
+    w = np.random.default_rng(11).normal(0, 0.5 / p.n, p.n)
+    check_eval(p, w, s)
+
+
+def test_eval_is_bit_reproducible_and_cache_independent(gpu):
+    """Cached neighbour lists change the clipping order, not the result."""
+    p = problems.make(1, g=48, res=192, beam=True)
+    w1 = np.random.default_rng(5).normal(0, 0.5 / p.n, p.n)
+    a = solver_for(p)
+    f1, mu1, _, _ = a.eval(w1)          # cold: window candidates
+    f2, mu2, _, _ = a.eval(w1)          # warm: cached neighbours
+    b = solver_for(p)
+    b.eval(np.zeros(p.n))               # cache from another point
+    f3, mu3, _, _ = b.eval(w1)
+    assert np.array_equal(mu1, mu2) and f1 == f2
+    assert np.abs(mu1 - mu3).max() <= 1e-13 * mu1.max()
+
+
+def test_large_instance_conservation(gpu):
+    """Config-2 shape at full size: size-independent properties."""
+    p = problems.make(2)
+    s = solver_for(p)
+    for w in (np.zeros(p.n), np.random.default_rng(2).normal(0, 0.5 / p.n, p.n)):
+        f, mu, g, _ = s.eval(w)
+        assert abs(mu.sum() - 1.0) < 1e-11
+        assert abs(g.sum()) < 1e-11
+        # adjacency is symmetric
+        off, xy, nb = s.cells(w)
+        pairs = set()
+        for i in range(p.n):
+            for j in nb[off[i]:off[i + 1]]:
+                if j >= 0:
+                    pairs.add((i, int(j)))
+        assert all((j, i) in pairs for (i, j) in pairs)
+    # directional derivative of f is g.d
+    w = np.random.default_rng(3).normal(0, 0.5 / p.n, p.n)
+    d = np.random.default_rng(4).normal(0, 1.0 / p.n, p.n)
+    eps = 1e-3
+    fp = s.eval(w + eps * d)[0]
+    fm = s.eval(w - eps * d)[0]
+    g = s.eval(w)[2]
+    assert abs((fp - fm) / (2 * eps) - g @ d) < 1e-6 * abs(g @ d) + 1e-12
+
+
+def test_wolfe_solve_matches_oracle(gpu):
+    p = problems.make(1, g=16, res=64)
+    s = solver_for(p)
+    w, st = s.solve(np.zeros(p.n), mode=capi.SOLVE_WOLFE, tol=1e-4, history=10)
+    ow, ost = O.lbfgs_wolfe(oracle_problem(p), np.zeros(p.n), tol=1e-4, m=10)
+    assert st.converged and ost.converged
+    assert st.iterations == ost.iterations and st.evaluations == ost.evaluations
+    # the two trajectories differ only by rounding (device reductions vs numpy
+    # sums); over ~160 iterations that moves the weights far less than the
+    # 1e-4 mass tolerance pins them (~1e-6 of their range)
+    assert np.abs(w - ow).max() < 1e-6 * np.abs(ow).max()
+    assert O.max_rel_error(O.evaluate(oracle_problem(p), w).mu, p.nu) <= 1e-4
+
+
+def test_reference_mode_solve_matches_oracle(gpu):
+    """direct_ot's loop (backtracking, stale ||g|| stop) against its restatement."""
+    p = problems.make(1, g=12, res=48)
+    s = solver_for(p)
+    w, st = s.solve(np.zeros(p.n), mode=capi.SOLVE_REFERENCE, tol=1e-5, history=7, max_iter=2000)
+    ow, ost = O.direct_ot_parity(oracle_problem(p), np.zeros(p.n), total_iter=2000, tol=1e-5, m=7)
+    assert st.converged and ost.converged
+    assert abs(st.iterations - ost.iterations) <= max(2, ost.iterations // 20)
+    e = O.evaluate(oracle_problem(p), w)
+    assert np.linalg.norm(e.g) < 2e-5
+
+
+def test_solve_reaches_tolerance_config1(gpu):
+    p = problems.make(1)
+    s = solver_for(p)
+    w, st = s.solve(np.zeros(p.n), mode=capi.SOLVE_WOLFE, tol=1e-4, history=10)
+    assert st.converged and st.max_rel_err <= 1e-4
+    mu = O.evaluate(oracle_problem(p), w).mu
+    assert O.max_rel_error(mu, p.nu) <= 1e-4 * (1 + 1e-6)
+    assert abs(w.sum()) < 1e-12 * np.abs(w).sum()   # sum(g) = 0 keeps sum(w) (up to rounding)
+
+
+def test_centroids_parity(gpu):
+    p = problems.make(1, g=24, res=96)
+    s = solver_for(p)
+    w = np.random.default_rng(7).normal(0, 0.6 / p.n, p.n)
+    c = O.cells(p.xy, w, O.proj_corner(p.xy, p.proj_domain))
+    for weighted in (True, False):
+        xy, ex = s.centroids(w, weighted=weighted)
+        oxy, oex = O.centers(c, p.picture, p.size, p.proj_domain, weighting=weighted)
+        assert np.array_equal(ex, oex)
+        assert np.abs(xy[ex] - oxy[ex]).max() < 1e-10
+
+
+def test_source_masses_parity(gpu):
+    pts = seeds.initial_xy_point(900, [0.0, 40.0, 0.0, 40.0])
+    s = capi.Solver()
+    nu = s.source_masses(pts, [0.0, 40.0, 0.0, 40.0])
+    onu = O.source_masses(pts, [0.0, 40.0, 0.0, 40.0])
+    assert abs(nu.sum() - 1600.0) < 1e-9
+    assert np.abs(nu - onu).max() < 1e-10 * onu.max()
+
+
+def test_torch_device_buffers(gpu):
+    import torch
+
+    p = problems.make(1, g=16, res=64)
+    s = capi.Solver()
+    dev = torch.device("cuda", 0)
+    s.set_problem(torch.from_numpy(p.xy.reshape(-1)).to(dev), torch.from_numpy(p.nu).to(dev),
+                  torch.from_numpy(p.picture).to(dev), p.size, p.proj_domain)
+    w = np.random.default_rng(1).normal(0, 0.3 / p.n, p.n)
+    f, mu, g, fc = s.eval(torch.from_numpy(w).to(dev))
+    ev = O.evaluate(oracle_problem(p), w)
+    assert np.abs(mu.cpu().numpy() - ev.mu).max() <= MU_TOL * ev.mu.max()
+    wd, st = s.solve(torch.zeros(p.n, dtype=torch.float64, device=dev), mode=capi.SOLVE_WOLFE, tol=1e-4)
+    assert st.converged and wd.is_cuda
+
+
+def test_tiny_and_degenerate_inputs(gpu):
+    """One site, two sites, sites on the domain boundary, a zero-density band."""
+    dom = problems.UNIT_DOMAIN
+    s = capi.Solver()
+    s.set_problem(np.array([[0.3, 0.4]]), np.array([1.0]), np.ones(16), (4, 4), dom)
+    f, mu, g, _ = s.eval(np.zeros(1))
+    assert abs(mu[0] - 1.0) < 1e-14
+    xy = np.array([[0.25, 0.5], [0.75, 0.5]])
+    s.set_problem(xy, np.array([0.5, 0.5]), np.ones(16), (4, 4), dom)
+    for dw in (0.0, 0.1, -0.05):
+        mu = s.eval(np.array([dw, 0.0]))[1]
+        assert abs(mu[0] - (0.5 + dw)) < 1e-14
+    # sites on the boundary and a density with an empty band
+    pts = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0], [0.5, 0.5], [0.0, 0.5]])
+    dens = np.ones((8, 8))
+    dens[3:5, :] = 0.0
+    nu = np.full(6, 1 / 6)
+    s.set_problem(pts, nu, dens.ravel(), (8, 8), dom)
+    w = np.array([0.0, 0.01, -0.01, 0.02, 0.0, 0.005])
+    mu = s.eval(w)[1]
+    prob = O.Problem(pts, nu, dens.ravel() / dens.sum(), (8, 8), dom)
+    ev = O.evaluate(prob, w)
+    assert np.abs(mu - ev.mu).max() < 1e-12
+
+
+def test_bad_arguments_are_reported(gpu):
+    s = capi.Solver()
+    with pytest.raises(capi.CotError) as e:
+        s.eval(np.zeros(4))
+    assert e.value.code == capi.COT_ENOPROBLEM
+    with pytest.raises(capi.CotError):
+        s.set_problem(np.zeros((2, 2)), np.array([1.0, -1.0]), np.ones(4), (2, 2), problems.UNIT_DOMAIN)
+    with pytest.raises(capi.CotError):
+        s.set_problem(np.zeros((2, 2)), np.ones(2), np.ones(4), (2, 2), [1.0, 0.0, 0.0, 1.0])
+
+
+def test_reference_run_on_gpu(gpu):
+    """The committed reference run through the GPU path: source masses,
+    masses at the converged weights and the weighted centroids."""
+    with open(os.path.join(GOLD, "run.json")) as f:
+        run = json.load(f)
+    pts = seeds.initial_xy_point(run["point_num"], run["sample_domain"])
+    proj = seeds.initial_proj_point(pts, run["sample_domain"], run["proj_domain"])
+    pic = np.load(os.path.join(GOLD, "ustc_centerL.npz"))["picture"]
+    dens, size = seeds.picture_from_matrix(pic)
+    with gzip.open(os.path.join(GOLD, "weights0.txt.gz"), "rt") as f:
+        w = np.loadtxt(f)
+    s = capi.Solver()
+    nu = s.source_masses(pts, run["sample_domain"])
+    onu = O.source_masses(pts, run["sample_domain"])
+    assert np.abs(nu - onu).max() < 1e-10 * onu.max()
+    s.set_problem(proj, nu, dens, size, run["proj_domain"])
+    f, mu, g, _ = s.eval(w)
+    assert (mu == 0).sum() == 0
+    assert np.linalg.norm(g) < 0.12
+    pn = O.normalize_picture(dens, run["sample_domain"])
+    ev = O.evaluate(O.Problem(proj, onu, pn, size, run["proj_domain"]), w)
+    assert np.abs(mu - ev.mu).max() < 1e-10 * ev.mu.max()
+    c, ex = s.centroids(w)
+    assert ex.all()
+    with gzip.open(os.path.join(GOLD, "out0_sub.txt.gz"), "rt") as f:
+        sub = [r.split() for r in f.read().splitlines() if not r.startswith("#")]
+    oi = np.array([int(a[0]) for a in sub])
+    ov = np.array([[float(a[1]), float(a[2])] for a in sub])
+    d = np.abs(c[oi] - ov)
+    assert np.median(d) < 5e-4 and np.percentile(d, 99) < 1e-2 and d.max() < 3e-2
