@@ -35,8 +35,9 @@ SOLVE_WOLFE = 1
 EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
-    "cot_last_error",
+    "cot_eval_summary_noalloc", "cot_last_error",
 ]
+NOALLOC_MAX_N = 2048 * 1024
 
 
 class cot_config(ctypes.Structure):
@@ -95,6 +96,7 @@ def load():
         L.cot_source_masses.argtypes = [vp, dp, ctypes.c_int, dp, dp]
         L.cot_render.argtypes = [vp, dp, ctypes.c_double, dp]
         L.cot_get_kernel_stats.argtypes = [vp, ctypes.POINTER(cot_kernel_stats), ctypes.c_int]
+        L.cot_eval_summary_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTED:
             getattr(L, name).restype = ctypes.c_int

@@ -174,6 +174,29 @@ COT_API int cot_source_masses(cot_handle *h, const double *points_xy, int n,
  * (ot_op.cuh:215).  out has nx*ny entries (host memory). */
 COT_API int cot_render(cot_handle *h, const double *w, double gray_multiple, double *out);
 
+/* Allocation-free evaluation summary.  No counterpart in the reference (its
+ * host code copies the per-cell arrays back and sums them on the CPU).
+ * For callers that may not call cudaMalloc where they need these numbers:
+ * code recording a CUDA stream capture (an allocation there breaks the
+ * capture) and hosts that give the library a fixed memory budget with no
+ * allocations after start-up.  Reduces per-cell results already on the
+ * device -- mu, f_cell, nu (n doubles each, device pointers, e.g. the outputs
+ * of cot_eval with COT_MEM_DEVICE) -- to out[0..3] (device) =
+ * {sum f_cell, max |mu - nu| / nu, sum (mu - nu)^2, count(mu == 0)}.
+ * Allocates nothing: its scratch is one fixed array per device
+ * (COT_NOALLOC_MAX_BLOCKS x 4 doubles + a counter, about 32 KB) that every
+ * GPU loading the library holds until exit; n above COT_NOALLOC_MAX_N is
+ * rejected with COT_EINVAL.  All calls share that array: calls that overlap
+ * on the GPU race, so order them on one stream.  The first call on a device
+ * looks the array's address up; make it before any stream capture starts.
+ * Errors are read with cot_last_error(NULL, ...). */
+#define COT_NOALLOC_BLOCK_ELEMS 2048
+#define COT_NOALLOC_MAX_BLOCKS 1024
+#define COT_NOALLOC_MAX_N (COT_NOALLOC_BLOCK_ELEMS * COT_NOALLOC_MAX_BLOCKS)
+#define COT_NOALLOC_MAX_DEVICES 64
+COT_API int cot_eval_summary_noalloc(const double *mu, const double *f_cell, const double *nu, int n,
+                                     double *out, void *cuda_stream);
+
 /* Kernel accounting since the last reset; waits for the handle's stream.
  * reset=1 clears the counters after reading. */
 COT_API int cot_get_kernel_stats(cot_handle *h, cot_kernel_stats *out, int reset);
