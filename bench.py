@@ -265,7 +265,7 @@ def run_ours(args):
     traffic = committed_traffic()
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-            "kernel": "k_cells<64> (fused power cell + pixel integration)",
+            "kernel": "k_cells_fast (fused power cell + pixel integration)",
             "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms, "launches": ks["cell_launches"],
             "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"}
 
