@@ -35,7 +35,7 @@ SOLVE_WOLFE = 1
 EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
-    "cot_eval_summary_noalloc", "cot_last_error",
+    "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_last_error",
 ]
 NOALLOC_MAX_N = 2048 * 1024
 
@@ -61,6 +61,13 @@ class cot_solve_stats(ctypes.Structure):
                 ("converged", ctypes.c_int), ("f", ctypes.c_double), ("max_rel_err", ctypes.c_double),
                 ("grad_norm", ctypes.c_double), ("empty_cells", ctypes.c_int),
                 ("ring_overflows", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
+class cot_aarl_inputs(ctypes.Structure):
+    _fields_ = [("points_xy", ctypes.c_void_p), ("input_light", ctypes.c_void_p), ("inside_light", ctypes.c_void_p),
+                ("height", ctypes.c_void_p), ("z_of_len", ctypes.c_double), ("z_of_receiver", ctypes.c_double),
+                ("refraction_index", ctypes.c_double), ("sample_domain", ctypes.c_double * 4),
+                ("aa_history", ctypes.c_int), ("aa_fixed_para", ctypes.c_double), ("lbfgs_prepass", ctypes.c_int)]
 
 
 class CotError(RuntimeError):
@@ -97,6 +104,8 @@ def load():
         L.cot_render.argtypes = [vp, dp, ctypes.c_double, dp]
         L.cot_get_kernel_stats.argtypes = [vp, ctypes.POINTER(cot_kernel_stats), ctypes.c_int]
         L.cot_eval_summary_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
+        L.cot_solve_aarl.argtypes = [vp, vp, ctypes.POINTER(cot_aarl_inputs), ctypes.POINTER(cot_solve_opts),
+                                     ctypes.POINTER(cot_solve_stats)]
         L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         for name in EXPORTED:
             getattr(L, name).restype = ctypes.c_int
@@ -258,6 +267,26 @@ class Solver:
         stats = SolveStats(st.iterations, st.evaluations, st.restarts, bool(st.converged), st.f, st.max_rel_err,
                            st.grad_norm, st.empty_cells, st.ring_overflows, st.ms)
         return w, stats
+
+    def solve_aarl(self, w0, points, input_light, inside_light, height, *, z_of_len, z_of_receiver,
+                   refraction_index, sample_domain, aa_history=7, aa_fixed_para=-2.0, lbfgs_prepass=True,
+                   history=7, max_iter=50001, tol=0.01, initial_step=1.0, raise_on_noconv=False):
+        """aarl_direct_ot: Fresnel-reweighted masses + Anderson acceleration.
+        The problem's masses must be the source masses; on return they are
+        the re-weighted ones.  Host arrays only."""
+        w = _f64(w0).copy()
+        keep = [_f64(points).reshape(-1), _f64(input_light).reshape(-1), _f64(inside_light).reshape(-1),
+                _f64(height).reshape(-1)]
+        ai = cot_aarl_inputs(keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data, keep[3].ctypes.data,
+                             z_of_len, z_of_receiver, refraction_index,
+                             (ctypes.c_double * 4)(*[float(v) for v in sample_domain]), aa_history, aa_fixed_para,
+                             int(bool(lbfgs_prepass)))
+        opts = cot_solve_opts(SOLVE_REFERENCE, history, max_iter, tol, initial_step, 0.0, 0.0, 0, 0)
+        st = cot_solve_stats()
+        rc = self._L.cot_solve_aarl(self._h, _vptr(w), ctypes.byref(ai), ctypes.byref(opts), ctypes.byref(st))
+        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV,))
+        return w, SolveStats(st.iterations, st.evaluations, st.restarts, bool(st.converged), st.f, st.max_rel_err,
+                             st.grad_norm, st.empty_cells, st.ring_overflows, st.ms)
 
     def centroids(self, w, weighted=True):
         if _is_torch(w):

@@ -554,7 +554,10 @@ extern "C" int cot_eval(cot_handle *h, const double *w, double *f_total, double 
     CotEvalOut o;
     COT_CUDA_TRY(cudaMemcpyAsync(&o, P.out, sizeof o, cudaMemcpyDeviceToHost, s));
     if (mu && (r = download_sorted(h, P.mut, mu, mem)) != COT_OK) return r;
-    if (f_cell && (r = download_sorted(h, P.fc, f_cell, mem)) != COT_OK) return r;
+    if (f_cell) {
+        launch_fcell_full(P.n, P.fc, P.wt, P.nu, P.d, h->c());
+        if ((r = download_sorted(h, P.d, f_cell, mem)) != COT_OK) return r;
+    }
     if (g) {
         k_grad<<<nblk(P.n), 256, 0, s>>>(P.n, P.mut, P.nu, P.d);
         if ((r = download_sorted(h, P.d, g, mem)) != COT_OK) return r;
@@ -717,20 +720,23 @@ extern "C" int cot_render(cot_handle *h, const double *w, double gray_multiple, 
 // ---------------------------------------------------------------------------
 // solve
 // ---------------------------------------------------------------------------
-extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts, cot_solve_stats *stats, int mem)
+// Options check shared by the solve entry points.
+static int check_opts(cot_handle *h, cot_solve_opts &o)
 {
-    if (!h) return COT_EINVAL;
-    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_solve: no problem set", nullptr);
-    if (!w_inout || !opts) return fail(h, COT_EINVAL, "cot_solve: NULL argument", nullptr);
-    cot_solve_opts o = *opts;
-    if (o.mode != COT_SOLVE_REFERENCE && o.mode != COT_SOLVE_WOLFE) return fail(h, COT_EINVAL, "cot_solve: bad mode", nullptr);
-    if (o.history <= 0 || o.history > COT_MAX_HIST) return failf(h, COT_EINVAL, "cot_solve: history must be in 1..%d", COT_MAX_HIST);
-    if (o.max_iter < 0) return fail(h, COT_EINVAL, "cot_solve: max_iter < 0", nullptr);
+    if (o.mode != COT_SOLVE_REFERENCE && o.mode != COT_SOLVE_WOLFE) return fail(h, COT_EINVAL, "solve: bad mode", nullptr);
+    if (o.history <= 0 || o.history > COT_MAX_HIST) return failf(h, COT_EINVAL, "solve: history must be in 1..%d", COT_MAX_HIST);
+    if (o.max_iter < 0) return fail(h, COT_EINVAL, "solve: max_iter < 0", nullptr);
     if (!(o.initial_step > 0)) o.initial_step = 1.0;
     if (!(o.c1 > 0)) o.c1 = 1e-4;
     if (!(o.c2 > 0)) o.c2 = 0.9;
     if (o.max_ls <= 0) o.max_ls = 30;
-    COT_CUDA_TRY(cudaSetDevice(h->device));
+    return COT_OK;
+}
+
+// Device L-BFGS from the weights in P.w (sorted order).  On return P.w holds
+// the last accepted point, P.mu its masses, and *out the control block.
+static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms)
+{
     CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
     const int n = P.n;
@@ -742,7 +748,7 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
         P.hist_alloc = 0;
         cudaError_t e = cudaMalloc(&P.Sv, (size_t)m * n * 8);
         if (e == cudaSuccess) e = cudaMalloc(&P.Yv, (size_t)m * n * 8);
-        if (e != cudaSuccess) return fail(h, COT_ENOMEM, "cot_solve: history allocation", cudaGetErrorString(e));
+        if (e != cudaSuccess) return fail(h, COT_ENOMEM, "solve: history allocation", cudaGetErrorString(e));
         P.hist_alloc = m;
     }
     COT_CUDA_TRY(cudaMemsetAsync(P.Sv, 0, (size_t)m * n * 8, s));
@@ -762,8 +768,6 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
     hs.f = INFINITY;
     if (o.max_iter == 0) hs.done = 1;
     COT_CUDA_TRY(cudaMemcpyAsync(P.S, &hs, sizeof(CotSolver), cudaMemcpyHostToDevice, s));
-    int r;
-    if ((r = upload_sorted(h, w_inout, mem, P.w)) != COT_OK) return r;
     cudaEvent_t e0, e1;
     COT_CUDA_TRY(cudaEventCreate(&e0));
     COT_CUDA_TRY(cudaEventCreate(&e1));
@@ -777,14 +781,13 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
         launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, h->c());
     }
     const size_t ctl = 16 * sizeof(int);
-    int guard = 0;
+    double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
     while (true) {
         launch_begin_iteration(P.S, h->c());
         launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, h->c());
         COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
         COT_CUDA_TRY(cudaStreamSynchronize(s));
         if (hs.done) break;
-        double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
         while (true) {
             CellsArgs a = cells_args(P, P.w, P.d, tptr);
             launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
@@ -792,7 +795,6 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
             COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
             COT_CUDA_TRY(cudaStreamSynchronize(s));
             if (!hs.ls_active) break;
-            if (++guard > 100000000) break;
         }
         if (hs.accepted)
             launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, h->c());
@@ -802,24 +804,293 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
     }
     COT_CUDA_TRY(cudaEventRecord(e1, s));
     COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
-    if ((r = download_sorted(h, P.w, w_inout, mem)) != COT_OK) return r;
     COT_CUDA_TRY(cudaStreamSynchronize(s));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms) *ms = t;
+    out = hs;
+    return COT_OK;
+}
+
+static void fill_stats(const CotSolver &hs, float ms, cot_solve_stats *stats)
+{
+    if (!stats) return;
+    stats->iterations = hs.iter;
+    stats->evaluations = hs.evals;
+    stats->restarts = hs.restarts;
+    stats->converged = hs.converged;
+    stats->f = hs.f;
+    stats->max_rel_err = hs.maxrel;
+    stats->grad_norm = std::sqrt(hs.gnorm2);
+    stats->empty_cells = hs.empty;
+    stats->ring_overflows = hs.ring_rejects;
+    stats->ms = ms;
+}
+
+extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts, cot_solve_stats *stats, int mem)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_solve: no problem set", nullptr);
+    if (!w_inout || !opts) return fail(h, COT_EINVAL, "cot_solve: NULL argument", nullptr);
+    cot_solve_opts o = *opts;
+    int r;
+    if ((r = check_opts(h, o)) != COT_OK) return r;
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    if ((r = upload_sorted(h, w_inout, mem, h->P.w)) != COT_OK) return r;
+    CotSolver hs;
+    float ms = 0;
+    if ((r = solve_device(h, o, hs, &ms)) != COT_OK) return r;
+    if ((r = download_sorted(h, h->P.w, w_inout, mem)) != COT_OK) return r;
+    COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    fill_stats(hs, ms, stats);
+    if (!hs.converged) return failf(h, COT_ENOTCONV, "cot_solve: stopped after %d iterations (max rel err %.3e)", hs.iter, hs.maxrel);
+    return COT_OK;
+}
+
+// Small symmetric positive system A a = 1 by LDL^T (A n x n, n <= 32).
+static bool ldlt_solve_ones(std::vector<double> A, int n, std::vector<double> &x)
+{
+    std::vector<double> L((size_t)n * n, 0.0), D(n, 0.0);
+    for (int j = 0; j < n; j++) {
+        double d = A[(size_t)j * n + j];
+        for (int k = 0; k < j; k++) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k] * D[k];
+        if (!(d != 0.0) || !std::isfinite(d)) return false;
+        D[j] = d;
+        L[(size_t)j * n + j] = 1.0;
+        for (int i = j + 1; i < n; i++) {
+            double v = A[(size_t)i * n + j];
+            for (int k = 0; k < j; k++) v -= L[(size_t)i * n + k] * L[(size_t)j * n + k] * D[k];
+            L[(size_t)i * n + j] = v / d;
+        }
+    }
+    x.assign(n, 1.0);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < i; k++) x[i] -= L[(size_t)i * n + k] * x[k];
+    for (int i = 0; i < n; i++) x[i] /= D[i];
+    for (int i = n - 1; i >= 0; i--)
+        for (int k = i + 1; k < n; k++) x[i] -= L[(size_t)k * n + i] * x[k];
+    for (double v : x)
+        if (!std::isfinite(v)) return false;
+    return true;
+}
+
+// Fresnel-reweighted Anderson solve: aarl_direct_ot (ot_op.cuh:591-1385).
+extern "C" int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inputs *in, const cot_solve_opts *opts,
+                              cot_solve_stats *stats)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_solve_aarl: no problem set", nullptr);
+    if (!w_inout || !in || !opts || !in->points_xy || !in->input_light || !in->inside_light || !in->height)
+        return fail(h, COT_EINVAL, "cot_solve_aarl: NULL argument", nullptr);
+    cot_solve_opts o = *opts;
+    o.mode = COT_SOLVE_REFERENCE;
+    int r;
+    if ((r = check_opts(h, o)) != COT_OK) return r;
+    const int M = in->aa_history;
+    if (M <= 0 || M > COT_MAX_HIST) return failf(h, COT_EINVAL, "cot_solve_aarl: aa_history must be in 1..%d", COT_MAX_HIST);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    const int n = P.n;
+    const size_t N = (size_t)n;
+    // sorted copies of the per-site inputs
+    const std::vector<int> &perm = P.hperm;
+    std::vector<double> src(2 * N), inl(3 * N), insl(3 * N), hgt(N);
+    for (size_t p = 0; p < N; p++) {
+        int i = perm[p];
+        src[2 * p] = in->points_xy[2 * (size_t)i];
+        src[2 * p + 1] = in->points_xy[2 * (size_t)i + 1];
+        for (int c = 0; c < 3; c++) {
+            inl[3 * p + c] = in->input_light[3 * (size_t)i + c];
+            insl[3 * p + c] = in->inside_light[3 * (size_t)i + c];
+        }
+        hgt[p] = in->height[i];
+    }
+    // device workspace of this call
+    double *dsrc = nullptr, *dinl = nullptr, *dinsl = nullptr, *dhgt = nullptr, *lam = nullptr, *energy = nullptr;
+    double *cen = nullptr, *G = nullptr, *F = nullptr, *row = nullptr, *coef = nullptr, *step = nullptr;
+    unsigned char *ex = nullptr;
+    auto release = [&]() {
+        void *ps[] = {dsrc, dinl, dinsl, dhgt, lam, energy, cen, G, F, row, coef, step, ex};
+        for (void *q : ps)
+            if (q) cudaFree(q);
+    };
+    cudaError_t e = cudaMalloc(&dsrc, 2 * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&dinl, 3 * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&dinsl, 3 * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&dhgt, N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&lam, N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&energy, N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&cen, 2 * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&ex, N);
+    if (e == cudaSuccess) e = cudaMalloc(&G, (size_t)M * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&F, (size_t)M * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&row, COT_MAX_HIST * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&coef, COT_MAX_HIST * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&step, 8);
+    if (e != cudaSuccess) {
+        release();
+        return fail(h, COT_ENOMEM, "cot_solve_aarl: device allocation", cudaGetErrorString(e));
+    }
+    auto cuda_fail = [&](const char *what, cudaError_t err) {
+        release();
+        return fail(h, COT_ECUDA, what, cudaGetErrorString(err));
+    };
+#define AARL_TRY(expr)                                  \
+    do {                                                \
+        cudaError_t e__ = (expr);                       \
+        if (e__ != cudaSuccess) return cuda_fail(#expr, e__); \
+    } while (0)
+    AARL_TRY(cudaMemcpyAsync(dsrc, src.data(), 2 * N * 8, cudaMemcpyHostToDevice, s));
+    AARL_TRY(cudaMemcpyAsync(dinl, inl.data(), 3 * N * 8, cudaMemcpyHostToDevice, s));
+    AARL_TRY(cudaMemcpyAsync(dinsl, insl.data(), 3 * N * 8, cudaMemcpyHostToDevice, s));
+    AARL_TRY(cudaMemcpyAsync(dhgt, hgt.data(), N * 8, cudaMemcpyHostToDevice, s));
+    // the problem's masses are the source masses lambda; they sum to area_scalar
+    AARL_TRY(cudaMemcpyAsync(lam, P.nu, N * 8, cudaMemcpyDeviceToDevice, s));
+    std::vector<double> hl(N);
+    AARL_TRY(cudaMemcpyAsync(hl.data(), lam, N * 8, cudaMemcpyDeviceToHost, s));
+    AARL_TRY(cudaStreamSynchronize(s));
+    double area_scalar = 0;
+    for (double v : hl) area_scalar += v;
+    if ((r = upload_sorted(h, w_inout, COT_MEM_HOST, P.w)) != COT_OK) {
+        release();
+        return r;
+    }
+    cudaEvent_t e0, e1;
+    AARL_TRY(cudaEventCreate(&e0));
+    AARL_TRY(cudaEventCreate(&e1));
+    AARL_TRY(cudaEventRecord(e0, s));
+    CotEvalOut ho{};
+    int evals = 0, iters = 0, restarts = 0, ring_rejects = 0;
+    // plain centroids at P.w + t*d -> Fresnel-weighted nu (ot_op.cuh:779-795, 1082-1092, 1212-1224);
+    // fills P.mut / P.fc / P.nv / P.wt for that point and reduces with the new nu
+    auto eval_with_nu = [&](const double *d, const double *tptr, bool update_nu) -> int {
+        CellsArgs a = cells_args(P, P.w, d, tptr);
+        a.cen = cen;
+        a.exist = ex;
+        a.weighted = 0;
+        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        evals++;
+        // ring check first (polygons_in_VD + the max_edge_num/2 test)
+        launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
+        cudaError_t err = cudaMemcpyAsync(&ho, P.out, sizeof ho, cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return -1;
+        if (ho.overflow > 0) return 1;
+        if (update_nu) {
+            launch_fresnel_nu(n, cen, dsrc, dinl, dinsl, dhgt, lam, in->z_of_len, in->z_of_receiver,
+                              in->refraction_index, area_scalar, energy, P.partials, P.nu, h->c());
+            launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
+            err = cudaMemcpyAsync(&ho, P.out, sizeof ho, cudaMemcpyDeviceToHost, s);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+            if (err != cudaSuccess) return -1;
+        }
+        return 0;
+    };
+    // 1. nu from the centroids at the warm start
+    if (eval_with_nu(nullptr, nullptr, true) < 0) return cuda_fail("cot_solve_aarl: first evaluation", cudaGetLastError());
+    // 2. optional L-BFGS pre-pass with nu fixed (ot_op.cuh:823-1074)
+    CotSolver pre{};
+    if (in->lbfgs_prepass) {
+        float pms = 0;
+        if ((r = solve_device(h, o, pre, &pms)) != COT_OK) {
+            release();
+            return r;
+        }
+        evals += pre.evals;
+        // 3. nu again from the centroids at the pre-pass result
+        if (eval_with_nu(nullptr, nullptr, true) < 0) return cuda_fail("cot_solve_aarl: evaluation", cudaGetLastError());
+    }
+    // current point: P.w, masses P.mut, nu in P.nu
+    AARL_TRY(cudaMemcpyAsync(P.mu, P.mut, N * 8, cudaMemcpyDeviceToDevice, s));
+    double f = ho.f, gnorm = std::sqrt(ho.gnorm2), maxrel = ho.maxrel;
+    int empty = ho.empty;
+    // 4. Anderson acceleration on w <- w + alpha g (ot_op.cuh:1112-1323)
+    std::vector<double> A((size_t)M * M, 0.0), hrow(M), a;
+    int aa_loop = 0;
+    bool converged = false;
+    for (int it = 0; it < o.max_iter; it++) {
+        iters = it + 1;
+        const int cnt = std::min(aa_loop + 1, M);
+        const int hidx = aa_loop % M;
+        const int empty_start = empty;
+        launch_aa_store_gram(n, P.w, P.mu, P.nu, in->aa_fixed_para, G, F, hidx, cnt, P.partials, P.ticket, row, h->c());
+        AARL_TRY(cudaMemcpyAsync(hrow.data(), row, cnt * 8, cudaMemcpyDeviceToHost, s));
+        AARL_TRY(cudaStreamSynchronize(s));
+        for (int j = 0; j < cnt; j++) A[(size_t)hidx * M + j] = A[(size_t)j * M + hidx] = hrow[j];
+        std::vector<double> As((size_t)cnt * cnt);
+        for (int i = 0; i < cnt; i++)
+            for (int j = 0; j < cnt; j++) As[(size_t)i * cnt + j] = A[(size_t)i * M + j] + (i == j ? 1e-10 : 0.0);
+        if (!ldlt_solve_ones(As, cnt, a)) {
+            release();
+            return fail(h, COT_ENOTCONV, "cot_solve_aarl: singular Anderson system", nullptr);
+        }
+        double sa = 0;
+        for (double v : a) sa += v;
+        for (double &v : a) v /= sa;
+        AARL_TRY(cudaMemcpyAsync(coef, a.data(), cnt * 8, cudaMemcpyHostToDevice, s));
+        launch_aa_combine(n, F, coef, cnt, P.w, P.d, h->c());
+        double t = 1.0;
+        bool accepted = false;
+        while (true) {
+            AARL_TRY(cudaMemcpyAsync(step, &t, 8, cudaMemcpyHostToDevice, s));
+            int rc = eval_with_nu(P.d, step, true);
+            if (rc < 0) return cuda_fail("cot_solve_aarl: evaluation", cudaGetLastError());
+            if (rc == 1) {
+                ring_rejects++;
+                t *= 0.5;
+            } else {
+                // accept unconditionally (ot_op.cuh:1206-1241)
+                AARL_TRY(cudaMemcpyAsync(P.w, P.wt, N * 8, cudaMemcpyDeviceToDevice, s));
+                AARL_TRY(cudaMemcpyAsync(P.mu, P.mut, N * 8, cudaMemcpyDeviceToDevice, s));
+                f = ho.f;
+                gnorm = std::sqrt(ho.gnorm2);
+                maxrel = ho.maxrel;
+                empty = ho.empty;
+                aa_loop++;
+                accepted = true;
+                break;
+            }
+            if (t <= 1e-4 * o.initial_step) break;
+        }
+        if (!accepted) {
+            aa_loop = 0;
+            restarts++;
+        }
+        // the reference counts empty cells (of the masses at the start of the
+        // iteration) only on every tenth iteration (ot_op.cuh:1256-1268)
+        const int check_degenerate = (it % 10 == 0) ? empty_start : 0;
+        if (gnorm < o.tol && check_degenerate == 0) {
+            converged = true;
+            break;
+        }
+    }
+    AARL_TRY(cudaEventRecord(e1, s));
+    if ((r = download_sorted(h, P.w, w_inout, COT_MEM_HOST)) != COT_OK) {
+        release();
+        return r;
+    }
+    AARL_TRY(cudaStreamSynchronize(s));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    release();
+#undef AARL_TRY
     if (stats) {
-        stats->iterations = hs.iter;
-        stats->evaluations = hs.evals;
-        stats->restarts = hs.restarts;
-        stats->converged = hs.converged;
-        stats->f = hs.f;
-        stats->max_rel_err = hs.maxrel;
-        stats->grad_norm = std::sqrt(hs.gnorm2);
-        stats->empty_cells = hs.empty;
-        stats->ring_overflows = hs.ring_rejects;
+        stats->iterations = iters;
+        stats->evaluations = evals;
+        stats->restarts = restarts;
+        stats->converged = converged ? 1 : 0;
+        stats->f = f;
+        stats->max_rel_err = maxrel;
+        stats->grad_norm = gnorm;
+        stats->empty_cells = empty;
+        stats->ring_overflows = ring_rejects;
         stats->ms = ms;
     }
-    if (!hs.converged) return failf(h, COT_ENOTCONV, "cot_solve: stopped after %d iterations (max rel err %.3e)", hs.iter, hs.maxrel);
+    if (!converged) return failf(h, COT_ENOTCONV, "cot_solve_aarl: stopped after %d iterations (|g| %.3e)", iters, gnorm);
     return COT_OK;
 }

@@ -1076,8 +1076,10 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
         }
         if (lane == 0) {
             a.mu[i] = acc.mu;
-            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941)
-            a.fc[i] = -wi * g.nu[i] - (acc.S - wi * acc.mu);
+            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941);
+            // stored without its -w_i nu_i term, which the reduction adds, so
+            // that nu may change after the cells are built
+            a.fc[i] = -(acc.S - wi * acc.mu);
             a.nv[i] = nv;
             if (a.cen != nullptr) {
                 const bool ex = nv >= 3;
@@ -1324,8 +1326,10 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
         }
         if (lane == 0) {
             a.mu[i] = acc.mu;
-            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941)
-            a.fc[i] = -wi * g.nu[i] - (acc.S - wi * acc.mu);
+            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941);
+            // stored without its -w_i nu_i term, which the reduction adds, so
+            // that nu may change after the cells are built
+            a.fc[i] = -(acc.S - wi * acc.mu);
             a.nv[i] = nv;
             if (a.cen != nullptr) {
                 bool ex = nv >= 3;

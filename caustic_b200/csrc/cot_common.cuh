@@ -125,7 +125,7 @@ struct CellsArgs {
     double *wt;            // trial weights out
     double *phibar;        // per bucket scratch
     double *mu;            // per cell mass out
-    double *fc;            // per cell objective out
+    double *fc;            // per cell objective out, without its -w_i nu_i term
     int *nv;               // per cell ring size out
     int *ovf_list;         // cells to redo with the large ring capacity
     int *ovf_count;        // device counters: [0] overflow count, [1..2] work
@@ -157,5 +157,12 @@ void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double
 void launch_reject(CotSolver *S, CotCtx &c);
 void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c);
 void configure_cells_kernels();
+void launch_fcell_full(int n, const double *fc, const double *wt, const double *nu, double *out, CotCtx &c);
+void launch_fresnel_nu(int n, const double *cen, const double *src, const double *inl, const double *insl,
+                       const double *hgt, const double *lam, double zl, double zr, double eta, double total,
+                       double *energy, double *partials, double *nu, CotCtx &c);
+void launch_aa_store_gram(int n, const double *w, const double *mu, const double *nu, double alpha, double *G,
+                          double *F, int h, int cnt, double *partials, unsigned int *ticket, double *row, CotCtx &c);
+void launch_aa_combine(int n, const double *F, const double *coef, int cnt, const double *w, double *d, CotCtx &c);
 
 }  // namespace cot

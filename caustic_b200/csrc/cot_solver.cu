@@ -119,6 +119,7 @@ __device__ void ls_decide(CotSolver *S, const CotEvalOut &o)
 // derivative; the last block finishes the sums and (in a solve) decides.
 __global__ void __launch_bounds__(RED_THREADS) k_reduce_eval(int n, const double *__restrict__ mu,
                                                             const double *__restrict__ fc, const int *__restrict__ nv,
+                                                            const double *__restrict__ wt,
                                                             const double *__restrict__ nu, const double *__restrict__ d,
                                                             int max_ring, double *partials, unsigned int *ticket,
                                                             CotEvalOut *out, CotSolver *S)
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_eval(int n, const double
     int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
     for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
         double g = mu[i] - nu[i];
-        f += fc[i];
+        f += fc[i] - wt[i] * nu[i];
         if (d != nullptr) gtd += g * d[i];
         double rel = nu[i] > 0.0 ? fabs(g) / nu[i] : (g != 0.0 ? INFINITY : 0.0);
         mx = fmax(mx, rel);
@@ -191,9 +192,8 @@ void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const in
                    const double *d, int max_ring, double *partials, unsigned int *ticket, CotEvalOut *out,
                    CotSolver *solver, CotCtx &c)
 {
-    (void)wt;
     int nb = reduce_blocks(g.n);
-    k_reduce_eval<<<nb, RED_THREADS, 0, c.s>>>(g.n, mu, fc, nv, g.nu, d, max_ring, partials, ticket, out, solver);
+    k_reduce_eval<<<nb, RED_THREADS, 0, c.s>>>(g.n, mu, fc, nv, wt, g.nu, d, max_ring, partials, ticket, out, solver);
     c.launches++;
 }
 
@@ -464,6 +464,185 @@ __global__ void k_init_from_eval(CotSolver *S, const CotEvalOut *out)
 void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c)
 {
     k_init_from_eval<<<1, 1, 0, c.s>>>(S, out);
+    c.launches++;
+}
+
+// ---------------------------------------------------------------------------
+// helpers of cot_eval and of the Fresnel-reweighted Anderson solve
+// ---------------------------------------------------------------------------
+
+// f_i with its -w_i nu_i term (the cell kernels store it without)
+__global__ void k_fcell_full(int n, const double *__restrict__ fc, const double *__restrict__ wt,
+                             const double *__restrict__ nu, double *__restrict__ out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = fc[i] - wt[i] * nu[i];
+}
+
+void launch_fcell_full(int n, const double *fc, const double *wt, const double *nu, double *out, CotCtx &c)
+{
+    k_fcell_full<<<(n + 255) / 256, 256, 0, c.s>>>(n, fc, wt, nu, out);
+    c.launches++;
+}
+
+// fresnel_T_unpolarized (basic_function.cuh:407-435)
+__device__ double fresnel_t(const double wi[3], const double wt[3], const double nrm[3], double eta_i, double eta_t)
+{
+    const double eps = 1e-12;
+    double ci = fabs(wi[0] * nrm[0] + wi[1] * nrm[1] + wi[2] * nrm[2]);
+    double ct = fabs(wt[0] * nrm[0] + wt[1] * nrm[1] + wt[2] * nrm[2]);
+    ci = fmin(1.0, fmax(0.0, ci));
+    ct = fmin(1.0, fmax(0.0, ct));
+    double ds = eta_i * ci + eta_t * ct;
+    double dp = eta_i * ct + eta_t * ci;
+    if (fabs(ds) < eps) ds = eps;
+    if (fabs(dp) < eps) dp = eps;
+    double rs = (eta_i * ci - eta_t * ct) / ds;
+    double rp = (eta_i * ct - eta_t * ci) / dp;
+    rs *= rs;
+    rp *= rp;
+    return 1.0 - 0.5 * (rs + rp);
+}
+
+__device__ void normalize3(double v[3])
+{
+    double nn = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (nn < 1e-12) {
+        v[0] = v[1] = v[2] = 0.0;
+        return;
+    }
+    v[0] /= nn;
+    v[1] /= nn;
+    v[2] /= nn;
+}
+
+// compute_energy_remain_rate (basic_function.cuh:437-494) times the source
+// mass: energy_i = lambda_i * T1_i * T2_i, from the cell centroids.
+__global__ void k_fresnel_energy(int n, const double *__restrict__ cen, const double *__restrict__ src,
+                                 const double *__restrict__ inl, const double *__restrict__ insl,
+                                 const double *__restrict__ hgt, const double *__restrict__ lam, double zl,
+                                 double zr, double eta, double *__restrict__ energy)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double p[3] = {src[2 * i], src[2 * i + 1], zl};
+    double wi[3] = {inl[3 * i], inl[3 * i + 1], inl[3 * i + 2]};
+    double ins[3] = {insl[3 * i], insl[3 * i + 1], insl[3 * i + 2]};
+    double op[3] = {p[0] + hgt[i] * ins[0], p[1] + hgt[i] * ins[1], p[2] + hgt[i] * ins[2]};
+    double wo[3] = {cen[2 * i] - op[0], cen[2 * i + 1] - op[1], zr - op[2]};
+    normalize3(wo);
+    double n2[3] = {eta * ins[0] - wo[0], eta * ins[1] - wo[1], eta * ins[2] - wo[2]};
+    normalize3(n2);
+    const double n1[3] = {0.0, 0.0, 1.0};
+    double t1 = fresnel_t(wi, ins, n1, 1.0, eta);
+    double t2 = fresnel_t(ins, wo, n2, eta, 1.0);
+    energy[i] = lam[i] * (t1 * t2);
+}
+
+// Fixed-order sum of x: block partials in block order; every block of the
+// scale kernel re-reduces the partials identically.
+__global__ void __launch_bounds__(RED_THREADS) k_sum_partials(int n, const double *__restrict__ x, double *partials)
+{
+    __shared__ double sh[33];
+    int per = (n + gridDim.x - 1) / gridDim.x;
+    int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    double v = 0.0;
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) v += x[i];
+    v = block_reduce<false>(v, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v;
+}
+
+// nu_i = energy_i / sum(energy) * total
+__global__ void k_scale_to_total(int n, const double *__restrict__ energy, const double *__restrict__ partials,
+                                 int nparts, double total, double *__restrict__ nu)
+{
+    double s = 0.0;
+    for (int k = 0; k < nparts; k++) s += partials[k];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) nu[i] = energy[i] / s * total;
+}
+
+void launch_fresnel_nu(int n, const double *cen, const double *src, const double *inl, const double *insl,
+                       const double *hgt, const double *lam, double zl, double zr, double eta, double total,
+                       double *energy, double *partials, double *nu, CotCtx &c)
+{
+    k_fresnel_energy<<<(n + 255) / 256, 256, 0, c.s>>>(n, cen, src, inl, insl, hgt, lam, zl, zr, eta, energy);
+    int nb = reduce_blocks(n);
+    k_sum_partials<<<nb, RED_THREADS, 0, c.s>>>(n, energy, partials);
+    k_scale_to_total<<<(n + 255) / 256, 256, 0, c.s>>>(n, energy, partials, nb, total, nu);
+    c.launches += 3;
+}
+
+// Anderson history slot h: G_h = mu - nu, F_h = w + alpha G_h
+// (storage + compute_fixed_function, ot_op.cuh:1139-1142)
+__global__ void k_aa_store(int n, const double *__restrict__ w, const double *__restrict__ mu,
+                           const double *__restrict__ nu, double alpha, double *__restrict__ gh,
+                           double *__restrict__ fh)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double g = mu[i] - nu[i];
+    gh[i] = g;
+    fh[i] = w[i] + alpha * g;
+}
+
+// row[j] = G_h . G_j for j < cnt (fixed order: block partials, last block sums)
+__global__ void __launch_bounds__(RED_THREADS) k_aa_gram_row(int n, const double *__restrict__ G, int h, int cnt,
+                                                            double *partials, unsigned int *ticket, double *row)
+{
+    __shared__ double sh[33];
+    __shared__ bool last;
+    int per = (n + gridDim.x - 1) / gridDim.x;
+    int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    const double *gh = G + (size_t)h * n;
+    for (int j = 0; j < cnt; j++) {
+        const double *gj = G + (size_t)j * n;
+        double v = 0.0;
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) v += gh[i] * gj[i];
+        v = block_reduce<false>(v, sh);
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * COT_MAX_HIST + j] = v;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned int t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        volatile double *p = partials;
+        for (int j = 0; j < cnt; j++) {
+            double r = 0.0;
+            for (unsigned b = 0; b < gridDim.x; b++) r += p[(size_t)b * COT_MAX_HIST + j];
+            row[j] = r;
+        }
+        *ticket = 0u;
+    }
+}
+
+void launch_aa_store_gram(int n, const double *w, const double *mu, const double *nu, double alpha, double *G,
+                          double *F, int h, int cnt, double *partials, unsigned int *ticket, double *row, CotCtx &c)
+{
+    k_aa_store<<<(n + 255) / 256, 256, 0, c.s>>>(n, w, mu, nu, alpha, G + (size_t)h * n, F + (size_t)h * n);
+    k_aa_gram_row<<<reduce_blocks(n), RED_THREADS, 0, c.s>>>(n, G, h, cnt, partials, ticket, row);
+    c.launches += 2;
+}
+
+// d = sum_j coef_j F_j - w   (compute_weighted_sum + compute_subtract, ot_op.cuh:1172-1173)
+__global__ void k_aa_combine(int n, const double *__restrict__ F, const double *__restrict__ coef, int cnt,
+                             const double *__restrict__ w, double *__restrict__ d)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int j = 0; j < cnt; j++) s += coef[j] * F[(size_t)j * n + i];
+    d[i] = s - w[i];
+}
+
+void launch_aa_combine(int n, const double *F, const double *coef, int cnt, const double *w, double *d, CotCtx &c)
+{
+    k_aa_combine<<<(n + 255) / 256, 256, 0, c.s>>>(n, F, coef, cnt, w, d);
     c.launches++;
 }
 

@@ -155,6 +155,33 @@ COT_API int cot_cells(cot_handle *h, const double *w, int *ring_offsets, double 
 COT_API int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts,
               cot_solve_stats *stats, int mem);
 
+/* Inputs of the Fresnel-reweighted solve (host arrays, caller order). */
+typedef struct {
+    const double *points_xy;     /* source (lens) sites, 2n */
+    const double *input_light;   /* incoming direction per site, 3n */
+    const double *inside_light;  /* refracted direction per site, 3n, unit */
+    const double *height;        /* lens thickness along inside_light, n */
+    double z_of_len, z_of_receiver, refraction_index;
+    double sample_domain[4];
+    int aa_history;              /* Anderson memory (aa_history_size) */
+    double aa_fixed_para;        /* step of the fixed-point map (aa_fixed_para) */
+    int lbfgs_prepass;           /* if_aa_op_initial: L-BFGS first, nu fixed */
+} cot_aarl_inputs;
+
+/* Solve of the later outer iterations: aarl_direct_ot (ot_op.cuh:591-1385).
+ * The target masses are the problem's masses (the source masses lambda)
+ * re-weighted by the Fresnel transmittance of each cell's light path
+ * (compute_energy_remain_rate, basic_function.cuh:437-494), evaluated at the
+ * plain cell centroids and renormalised to the same total; they change with
+ * the weights.  Optional L-BFGS pre-pass with the masses fixed (opts: the
+ * reference's history_size, total_iter, convergence_tolerance,
+ * initial_step), then Anderson acceleration of w <- w + aa_fixed_para * g,
+ * stopped when ||mu - nu||_2 < tol (empty cells checked every tenth
+ * iteration, as the reference).  On return the problem's masses are the
+ * re-weighted ones.  w_inout in host memory. */
+COT_API int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inputs *in,
+                           const cot_solve_opts *opts, cot_solve_stats *stats);
+
 /* Density-weighted (weighted=1) or plain centroids of the cells at w and
  * the exist flags.  Replaces compute_center (basic_function.cuh:1056-1191,
  * ot_op.cuh:539-546). */

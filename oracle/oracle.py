@@ -531,3 +531,111 @@ def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0
             k += 1
         st.iterations = it + 1
     return w, st
+
+
+# --------------------------------------------------------------------------
+# aarl_direct_ot (ot_op.cuh:591-1385)
+# --------------------------------------------------------------------------
+def _normalize3(v):
+    n = np.linalg.norm(v, axis=-1, keepdims=True)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        out = np.where(n < 1e-12, 0.0, v / n)
+    return out
+
+
+def _fresnel_t(wi, wt, nrm, eta_i, eta_t):
+    """fresnel_T_unpolarized, basic_function.cuh:407-435 (rows of vectors)."""
+    eps = 1e-12
+    ci = np.clip(np.abs((wi * nrm).sum(-1)), 0.0, 1.0)
+    ct = np.clip(np.abs((wt * nrm).sum(-1)), 0.0, 1.0)
+    ds = eta_i * ci + eta_t * ct
+    dp = eta_i * ct + eta_t * ci
+    ds = np.where(np.abs(ds) < eps, eps, ds)
+    dp = np.where(np.abs(dp) < eps, eps, dp)
+    rs = ((eta_i * ci - eta_t * ct) / ds) ** 2
+    rp = ((eta_i * ct - eta_t * ci) / dp) ** 2
+    return 1.0 - 0.5 * (rs + rp)
+
+
+def energy_remain_rate(points, z_len, input_light, inside_light, height, out_points, z_recv, eta):
+    """compute_energy_remain_rate, basic_function.cuh:437-494."""
+    pts = _f64(points).reshape(-1, 2)
+    n = pts.shape[0]
+    p = np.column_stack([pts, np.full(n, z_len)])
+    wi = _f64(input_light).reshape(-1, 3)
+    ins = _f64(inside_light).reshape(-1, 3)
+    op = p + _f64(height)[:, None] * ins
+    rec = np.column_stack([_f64(out_points).reshape(-1, 2), np.full(n, z_recv)])
+    wt = _normalize3(rec - op)
+    n2 = _normalize3(eta * ins - wt)
+    n1 = np.tile([0.0, 0.0, 1.0], (n, 1))
+    return _fresnel_t(wi, ins, n1, 1.0, eta) * _fresnel_t(ins, wt, n2, eta, 1.0)
+
+
+def aarl_direct_ot(prob: Problem, w0, lam, points, input_light, inside_light, height, z_len, z_recv, eta,
+                   aa_history=7, aa_fixed_para=-2.0, prepass=True, total_iter=50001, tol=0.01, m=7,
+                   initial_step=1.0, max_ring=200):
+    """Restatement of aarl_direct_ot.  lam: source masses (sum = area_scalar).
+    Cells that do not exist take their site as the centroid (the reference
+    reads whatever the centroid buffer held there)."""
+    lam = _f64(lam)
+    total = lam.sum()
+    st = SolveStats()
+
+    def nu_at(w):
+        c = cells(prob.xy, w, prob.box, prob.cap)
+        ctr, ex = centers(c, prob.picture, prob.size, prob.pd, weighting=False)
+        ctr = np.where(ex[:, None], ctr, prob.xy)
+        e = lam * energy_remain_rate(points, z_len, input_light, inside_light, height, ctr, z_recv, eta)
+        return e / e.sum() * total, c
+
+    w = _f64(w0).copy()
+    prob.nu, _ = nu_at(w)
+    if prepass:
+        w, pre = direct_ot_parity(prob, w, total_iter=total_iter, tol=tol, initial_step=initial_step, m=m,
+                                  max_ring=max_ring)
+        st.evaluations += pre.evaluations
+        prob.nu, _ = nu_at(w)
+    ev = evaluate(prob, w)
+    mu, g = ev.mu, ev.g
+    M = aa_history
+    n = w.shape[0]
+    Gh = np.zeros((M, n))
+    Fh = np.zeros((M, n))
+    aa = 0
+    for it in range(total_iter):
+        cnt = min(aa + 1, M)
+        h = aa % M
+        empty_start = int((mu == 0).sum())
+        Gh[h] = g
+        Fh[h] = w + aa_fixed_para * g
+        A = Gh[:cnt] @ Gh[:cnt].T + 1e-10 * np.eye(cnt)
+        a = np.linalg.solve(A, np.ones(cnt))
+        a = a / a.sum()
+        d = a @ Fh[:cnt] - w
+        t = 1.0
+        acc = False
+        while True:
+            wt = w + t * d
+            c = cells(prob.xy, wt, prob.box, prob.cap)
+            st.evaluations += 1
+            if c.ring_len.max() > max_ring or (c.ring_len < 0).any():
+                t *= 0.5
+            else:
+                prob.nu, _ = nu_at(wt)
+                mu_t, _ = eval_cells(c, prob.xy, wt, prob.nu, prob.picture, prob.size, prob.pd)
+                w, mu, g = wt, mu_t, mu_t - prob.nu
+                aa += 1
+                acc = True
+                break
+            if t <= 1e-4 * initial_step:
+                break
+        if not acc:
+            aa = 0
+            st.restarts += 1
+        st.iterations = it + 1
+        check = empty_start if it % 10 == 0 else 0
+        if np.linalg.norm(g) < tol and check == 0:
+            st.converged = True
+            break
+    return w, prob.nu.copy(), st
