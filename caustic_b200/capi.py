@@ -207,6 +207,7 @@ class Solver:
     def set_problem(self, xy, nu, density, size, proj_domain):
         """size = (nx, ny): pixels along x and y, density[ix + iy*nx]."""
         nx, ny = int(size[0]), int(size[1])
+        self._size = (nx, ny)
         pd = _f64(proj_domain)
         if _is_torch(xy):
             self._check(self._L.cot_set_problem(self._h, _tptr(xy), _tptr(nu), int(nu.numel()), _tptr(density),
@@ -302,6 +303,14 @@ class Solver:
         rc = self._L.cot_centroids(self._h, _vptr(w), _vptr(xy), _vptr(ex), int(bool(weighted)), COT_MEM_HOST)
         self._check(rc)
         return xy, ex.astype(bool)
+
+    def render(self, w, gray_multiple=1.0, size=None):
+        """render (basic_function.cuh:660-741): nu spread over the pixels,
+        times gray_multiple; returns density-layout array nx*ny."""
+        w = _f64(w)
+        out = np.zeros(int(self._size[0]) * int(self._size[1]))
+        self._check(self._L.cot_render(self._h, _dptr(w), float(gray_multiple), _dptr(out)))
+        return out
 
     def source_masses(self, points, sample_domain):
         p = _f64(points).reshape(-1, 2)

@@ -97,6 +97,65 @@ static bool read_picture(const std::string &path, std::vector<double> &data, int
 
 static void ensure_parent(const std::string &p) { fs::create_directories(fs::path(p).parent_path()); }
 
+// writeOBJ (basic_function.cuh:15-59): one face per cell with >= 3 vertices
+// (the rings here are the cells inside proj_domain)
+static bool write_obj(cot_handle *h, const std::vector<double> &w, const std::string &path)
+{
+    const int n = (int)w.size();
+    std::vector<int> off(n + 1);
+    int cap = 16 * n + 64;
+    std::vector<double> xy;
+    std::vector<int> nb;
+    for (int tries = 0; tries < 6; tries++) {
+        xy.resize(2 * (size_t)cap);
+        nb.resize(cap);
+        int rc = cot_cells(h, w.data(), off.data(), xy.data(), nb.data(), cap);
+        if (rc == COT_OK) break;
+        if (rc != COT_ECAPACITY) return false;
+        cap *= 2;
+    }
+    ensure_parent(path);
+    std::ofstream f(path);
+    if (!f) return false;
+    int g = 1;
+    for (int i = 0; i < n; i++) {
+        int a = off[i], b = off[i + 1];
+        if (b - a < 3) continue;
+        for (int k = a; k < b; k++) f << "v " << xy[2 * k] << " " << xy[2 * k + 1] << " 0.0\n";
+        f << "f ";
+        for (int k = a; k < b; k++) f << g++ << " ";
+        f << "\n";
+    }
+    return true;
+}
+
+// save_array_to_txt (basic_function.cuh:205-248): fixed, 6 decimals, rows of x from the top
+static bool write_render(cot_handle *h, const std::vector<double> &w, double gray, int m, int nn, const std::string &path)
+{
+    std::vector<double> img((size_t)m * nn);
+    if (cot_render(h, w.data(), gray, img.data()) != COT_OK) return false;
+    ensure_parent(path);
+    std::ofstream f(path);
+    if (!f) return false;
+    char buf[64];
+    for (int row = 0; row < m; row++) {
+        for (int col = 0; col < nn; col++) {
+            std::snprintf(buf, sizeof buf, "%.6f", img[(size_t)col * m + (m - 1 - row)]);
+            f << buf;
+            if (col != nn - 1) f << " ";
+        }
+        f << "\n";
+    }
+    return true;
+}
+
+static void write_weights_file(const std::vector<double> &w, const std::string &path)
+{
+    ensure_parent(path);
+    std::ofstream f(path);
+    for (double v : w) f << v << std::endl;
+}
+
 static int solver_error(cot_handle *h, const char *what)
 {
     char buf[512];
@@ -254,6 +313,19 @@ int main(int argc, char *argv[])
     if (cot_set_problem(h, proj_xy.data(), nu.data(), n, picture.data(), pm, pn, proj_domain.data(), COT_MEM_HOST) != COT_OK)
         return solver_error(h, "cot_set_problem");
 
+    // diagnostics of the reference (ot_op.cuh:214-219, 281-286): the starting cells
+    double raw_sum = 0;
+    for (double v : picture) raw_sum += v;
+    const double area_scalar = (sample_domain[1] - sample_domain[0]) * (sample_domain[3] - sample_domain[2]);
+    const double gray = raw_sum / area_scalar;
+    const std::string render_dir = "../render_result/" + xiushi + "/" + ot_time + "/";
+    const std::string mesh_dir = "../mesh_output/" + xiushi + "/" + ot_time + "/";
+    const std::string wdir = "../weights/" + xiushi + "/" + ot_time + "/";
+    const std::string pre = ot_time == "0" ? "" : "pre_";
+    if (!write_render(h, w, gray, pm, pn, render_dir + pre + "render_initial.txt") ||
+        !write_obj(h, w, mesh_dir + (ot_time == "0" ? "mesh_initial.obj" : "pre_initial_mesh.obj")))
+        std::cerr << "could not write the initial diagnostics" << std::endl;
+
     cot_solve_opts o{};
     o.mode = COT_SOLVE_REFERENCE;
     o.history = history_size;
@@ -285,6 +357,15 @@ int main(int argc, char *argv[])
     if (rc != COT_OK && rc != COT_ENOTCONV) return solver_error(h, "solve");
     std::cout << "iterations " << st.iterations << ", evaluations " << st.evaluations << ", |g| " << st.grad_norm
               << ", max rel " << st.max_rel_err << ", converged " << st.converged << ", " << st.ms << " ms" << std::endl;
+    // diagnostics at the end (ot_op.cuh:510-535, 1296-1321)
+    {
+        const std::string tag = (ot_time == "0" ? "" : ot_time + "_") + std::string("");
+        const std::string it = std::to_string(st.iterations > 0 ? st.iterations - 1 : 0);
+        write_weights_file(w, wdir + tag + "weights_" + it + ".txt");
+        if (!write_obj(h, w, mesh_dir + tag + "mesh_" + it + ".obj") ||
+            !write_render(h, w, gray, pm, pn, render_dir + tag + "render_" + it + ".txt"))
+            std::cerr << "could not write the final diagnostics" << std::endl;
+    }
     std::vector<double> cen(2 * (size_t)n);
     std::vector<unsigned char> ex(n);
     if (cot_centroids(h, w.data(), cen.data(), ex.data(), 1, COT_MEM_HOST) != COT_OK) return solver_error(h, "cot_centroids");

@@ -710,11 +710,29 @@ extern "C" int cot_source_masses(cot_handle *h, const double *points_xy, int n, 
 
 extern "C" int cot_render(cot_handle *h, const double *w, double gray_multiple, double *out)
 {
-    (void)w;
-    (void)gray_multiple;
-    (void)out;
     if (!h) return COT_EINVAL;
-    return fail(h, COT_EINVAL, "cot_render: not available in this build", nullptr);
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_render: no problem set", nullptr);
+    if (!w || !out) return fail(h, COT_EINVAL, "cot_render: NULL argument", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    const size_t npx = (size_t)P.geo.nx * P.geo.ny;
+    double *img = nullptr;
+    COT_CUDA_TRY(cudaMalloc(&img, npx * 8));
+    int r = upload_sorted(h, w, COT_MEM_HOST, P.w);
+    cudaError_t e = cudaMemsetAsync(img, 0, npx * 8, s);
+    if (r == COT_OK && e == cudaSuccess) {
+        CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+        a.splat = img;
+        a.splat_scale = gray_multiple;
+        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        e = cudaMemcpyAsync(out, img, npx * 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    cudaFree(img);
+    if (r != COT_OK) return r;
+    if (e != cudaSuccess) return fail(h, COT_ECUDA, "cot_render", cudaGetErrorString(e));
+    return COT_OK;
 }
 
 // ---------------------------------------------------------------------------

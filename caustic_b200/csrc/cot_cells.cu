@@ -461,6 +461,8 @@ struct PixGeo {
     const double *rho;
     double pd0, pd2, xs, ys, ixs, iys;
     int nx, ny;
+    double *splat;   // render: out[pix] += splat_w * area(cell ∩ pix) (nullable)
+    double splat_w;
 };
 
 __device__ __forceinline__ PixGeo pix_geo(const CotGeo &g)
@@ -475,6 +477,30 @@ __device__ __forceinline__ PixGeo pix_geo(const CotGeo &g)
     p.iys = g.iys;
     p.nx = g.nx;
     p.ny = g.ny;
+    p.splat = nullptr;
+    p.splat_w = 0.0;
+    return p;
+}
+
+// render (basic_function.cuh:660-741): the cell's carried mass spread over
+// the pixels in proportion to area; the weight is nu_i * gray / area(cell).
+template <class SP>
+__device__ PixGeo splat_geo(const CotGeo &g, const CellsArgs &a, const SP &P, int nv, int i, int lane)
+{
+    PixGeo p = pix_geo(g);
+    if (a.splat == nullptr) return p;
+    double ar = 0.0;
+    for (int k = lane; k < nv; k += 32) {
+        int kn = (k + 1 == nv) ? 0 : k + 1;
+        ar += P.X[k] * P.Y[kn] - P.X[kn] * P.Y[k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ar += __shfl_xor_sync(0xffffffffu, ar, o);
+    ar = 0.5 * fabs(ar);
+    if (ar != 0.0) {
+        p.splat = a.splat;
+        p.splat_w = g.nu[i] * a.splat_scale / ar;
+    }
     return p;
 }
 
@@ -601,6 +627,7 @@ __device__ __noinline__ CellAcc integrate_cell(SP &P, int nv, const PixGeo g, do
                 }
             }
             if (!(m.A > 0.0)) continue;
+            if (g.splat != nullptr) atomicAdd(g.splat + ix + iy * g.nx, g.splat_w * m.A);
             double rho = g.rho[ix + iy * g.nx];
             mu += rho * m.A;
             S += rho * (m.A * (xc * xc + yc * yc) + 2.0 * (xc * m.Ia + yc * m.Ib) + m.I2);
@@ -1054,7 +1081,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
         if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
         __syncwarp();
         CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (nv >= 3) acc = integrate_cell(S, nv, pix_geo(g), si, lane);
+        if (nv >= 3) acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
         PSTAT_CLOCK(t3);
         PSTAT_ADD(2, t3 - t2);
         PSTAT_ADD(8, 1);
@@ -1300,7 +1327,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
         PSTAT_CLOCK(t2);
         PSTAT_ADD(1, t2 - t1);
         CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (nv >= 3) acc = integrate_cell(P, nv, pix_geo(g), si, lane);
+        if (nv >= 3) acc = integrate_cell(P, nv, splat_geo(g, a, P, nv, i, lane), si, lane);
         PSTAT_CLOCK(t3);
         PSTAT_ADD(2, t3 - t2);
         PSTAT_ADD(8, 1);

@@ -135,6 +135,8 @@ struct CellsArgs {
     double *cen;           // centroids (nullable)
     unsigned char *exist;  // exist flags (nullable)
     int weighted;          // centroid flavour
+    double *splat;         // render output, nx*ny (nullable)
+    double splat_scale;    // gray_multiple of the render
     double *ring_xy;       // optional fixed-stride ring dump (nullable)
     int *ring_lab;
     int ring_cap;

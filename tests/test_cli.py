@@ -106,6 +106,14 @@ def test_file_contract_first_and_second_outer_iteration(gpu, cli, tmp_path):
     c, ex = O.centers(e.cells, O.normalize_picture(dens, sd), size, pd)
     assert np.abs(out - c[ex]).max() < 0.05
     assert os.path.exists(os.path.join(root, "data", "point_data", XIUSHI, "0", "_py_sp_settings.json"))
+    # diagnostics beside the build directory (ot_op.cuh:214-219, 281-286, 510-535)
+    ot = os.path.join(root, "Optimal_Transport_rl")
+    img = np.loadtxt(os.path.join(ot, "render_result", XIUSHI, "0", "render_initial.txt"))
+    assert img.shape == pic.shape and abs(img.sum() - pic.sum()) < 1e-3 * pic.sum()
+    with open(os.path.join(ot, "mesh_output", XIUSHI, "0", "mesh_initial.obj")) as f:
+        faces = [ln for ln in f if ln.startswith("f ")]
+    assert len(faces) == len(pts)
+    assert any(fn.startswith("weights_") for fn in os.listdir(os.path.join(ot, "weights", XIUSHI, "0")))
     # second outer iteration: warm start + Fresnel-reweighted Anderson solve
     r = subprocess.run([cli, "1", XIUSHI], cwd=build_dir, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr

@@ -170,6 +170,20 @@ def test_centroids_parity(gpu):
         assert np.abs(xy[ex] - oxy[ex]).max() < 1e-10
 
 
+def test_render_parity(gpu):
+    """render (basic_function.cuh:660-741): nu spread over the pixels."""
+    p = problems.make(1, g=20, res=80)
+    s = solver_for(p)
+    w = np.random.default_rng(9).normal(0, 0.5 / p.n, p.n)
+    img = s.render(w, gray_multiple=1.0)
+    c = O.cells(p.xy, w, O.proj_corner(p.xy, p.proj_domain))
+    ref = O.render(c, p.nu, p.size, p.proj_domain)
+    mu = s.eval(w)[1]
+    assert abs(img.sum() - p.nu[mu > 0].sum()) < 1e-12   # hidden cells carry nothing
+    assert np.abs(img - ref).max() < MU_TOL * ref.max()   # atomic accumulation order differs
+    assert np.abs(s.render(w, gray_multiple=3.0) - 3.0 * img).max() < 1e-12 * img.max()
+
+
 def test_source_masses_parity(gpu):
     pts = seeds.initial_xy_point(900, [0.0, 40.0, 0.0, 40.0])
     s = capi.Solver()
