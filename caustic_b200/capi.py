@@ -35,7 +35,7 @@ SOLVE_WOLFE = 1
 EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
-    "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_last_error",
+    "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_source_masses_point_light", "cot_last_error",
 ]
 NOALLOC_MAX_N = 2048 * 1024
 
@@ -101,6 +101,7 @@ def load():
         L.cot_solve.argtypes = [vp, vp, ctypes.POINTER(cot_solve_opts), ctypes.POINTER(cot_solve_stats), ctypes.c_int]
         L.cot_centroids.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int]
         L.cot_source_masses.argtypes = [vp, dp, ctypes.c_int, dp, dp]
+        L.cot_source_masses_point_light.argtypes = [vp, dp, ctypes.c_int, dp, dp, ctypes.c_double, dp]
         L.cot_render.argtypes = [vp, dp, ctypes.c_double, dp]
         L.cot_get_kernel_stats.argtypes = [vp, ctypes.POINTER(cot_kernel_stats), ctypes.c_int]
         L.cot_eval_summary_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
@@ -312,10 +313,17 @@ class Solver:
         self._check(self._L.cot_render(self._h, _dptr(w), float(gray_multiple), _dptr(out)))
         return out
 
-    def source_masses(self, points, sample_domain):
+    def source_masses(self, points, sample_domain, light=None, z_of_len=0.0):
+        """Parallel light (light=None): cell areas; a point light: the solid
+        angles of the cells seen from `light`; both normalised to the sample
+        domain's area."""
         p = _f64(points).reshape(-1, 2)
         out = np.empty(p.shape[0])
-        rc = self._L.cot_source_masses(self._h, _dptr(p), p.shape[0], _dptr(_f64(sample_domain)), _dptr(out))
+        if light is None:
+            rc = self._L.cot_source_masses(self._h, _dptr(p), p.shape[0], _dptr(_f64(sample_domain)), _dptr(out))
+        else:
+            rc = self._L.cot_source_masses_point_light(self._h, _dptr(p), p.shape[0], _dptr(_f64(sample_domain)),
+                                                       _dptr(_f64(light)), float(z_of_len), _dptr(out))
         self._check(rc)
         return out
 

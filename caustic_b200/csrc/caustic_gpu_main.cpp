@@ -18,7 +18,7 @@
 // Exit status: 0 done (also when the iteration cap is reached, as the
 // reference); 1 usage (as the reference); 255 unreadable JSON (the
 // reference's `return -1`); 2 a light/height file is missing; 3 a key is
-// missing or of the wrong type; 4 unsupported light type; 5 an input file is
+// missing or of the wrong type; 4 unknown light type; 5 an input file is
 // malformed; 6 the solver failed (CUDA error, bad problem).
 #include "causticot.h"
 #include "json_min.hpp"
@@ -299,17 +299,17 @@ int main(int argc, char *argv[])
             }
         }
     }
-    if (light_type != "parallel_light") {
-        std::cerr << "light_type point_light: solid-angle source masses are not available in this build" << std::endl;
-        return 4;
-    }
-
     cot_config cfg{};
     cot_handle *h = nullptr;
     if (cot_create(&cfg, &h) != COT_OK) return solver_error(nullptr, "cot_create");
     std::vector<double> nu(n);
-    if (cot_source_masses(h, points.data(), n, sample_domain.data(), nu.data()) != COT_OK)
-        return solver_error(h, "cot_source_masses");
+    if (light_type == "parallel_light") {
+        if (cot_source_masses(h, points.data(), n, sample_domain.data(), nu.data()) != COT_OK)
+            return solver_error(h, "cot_source_masses");
+    } else if (cot_source_masses_point_light(h, points.data(), n, sample_domain.data(), point_light.data(), z_of_len,
+                                             nu.data()) != COT_OK) {
+        return solver_error(h, "cot_source_masses_point_light");
+    }
     if (cot_set_problem(h, proj_xy.data(), nu.data(), n, picture.data(), pm, pn, proj_domain.data(), COT_MEM_HOST) != COT_OK)
         return solver_error(h, "cot_set_problem");
 

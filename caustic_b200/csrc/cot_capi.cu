@@ -671,13 +671,14 @@ extern "C" int cot_centroids(cot_handle *h, const double *w, double *xy, unsigne
     return COT_OK;
 }
 
-extern "C" int cot_source_masses(cot_handle *h, const double *points_xy, int n, const double sample_domain[4],
-                                 double *nu_out)
+// Source masses of the reference (ot_op.cuh:90-92,156-206): cells of the
+// source points (weights 0) inside the sample domain; parallel light weighs
+// them by area (compute_clip_area), a point light by the solid angle they
+// subtend from the light (solid_angle, basic_function.cuh:635-650);
+// normalised to total area_scalar.
+static int source_masses_impl(cot_handle *h, const double *points_xy, int n, const double *sd, const double *light,
+                              double z, double *nu_out)
 {
-    if (!h) return COT_EINVAL;
-    if (!points_xy || n <= 0 || !sample_domain || !nu_out) return fail(h, COT_EINVAL, "cot_source_masses: bad argument", nullptr);
-    const double *sd = sample_domain;
-    if (!(sd[1] > sd[0]) || !(sd[3] > sd[2])) return fail(h, COT_EINVAL, "cot_source_masses: empty sample_domain", nullptr);
     COT_CUDA_TRY(cudaSetDevice(h->device));
     // unweighted cells inside the sample domain, one "pixel" of unit density
     std::vector<double> xy(points_xy, points_xy + 2 * (size_t)n), one(n, 1.0), dens(1, 1.0);
@@ -685,27 +686,56 @@ extern "C" int cot_source_masses(cot_handle *h, const double *points_xy, int n, 
     int r = build_problem(h, Q, xy, one, dens, 1, 1, sd);
     if (r != COT_OK) return r;
     cudaStream_t s = h->stream;
-    std::vector<double> area(n), sorted(n);
+    std::vector<double> val(n), sorted(n);
+    double *solid = nullptr;
     cudaError_t e = cudaMemsetAsync(Q.w, 0, (size_t)n * 8, s);
+    if (e == cudaSuccess && light) e = cudaMalloc(&solid, (size_t)n * 8);
     if (e == cudaSuccess) {
         CellsArgs a = cells_args(Q, Q.w, nullptr, nullptr);
+        if (light) {
+            a.solid = solid;
+            a.solid_z = z;
+            for (int c = 0; c < 3; c++) a.solid_light[c] = light[c];
+        }
         launch_eval(Q.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
-        e = cudaMemcpyAsync(sorted.data(), Q.mut, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+        e = cudaMemcpyAsync(sorted.data(), light ? solid : Q.mut, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (solid) cudaFree(solid);
     std::vector<int> perm = Q.hperm;
     free_problem(Q);
     if (e != cudaSuccess) return fail(h, COT_ECUDA, "cot_source_masses", cudaGetErrorString(e));
-    // the density above integrates to n over the domain: rho = n / area; undo
     const double dom = (sd[1] - sd[0]) * (sd[3] - sd[2]);
+    // parallel light: the unit "pixel" integrates to n over the domain, so
+    // mu = n * area / dom; a point light: the solid angles themselves
+    for (int p = 0; p < n; p++) val[perm[p]] = light ? sorted[p] : sorted[p] * dom / (double)n;
     double tot = 0;
-    for (int p = 0; p < n; p++) {
-        area[perm[p]] = sorted[p] * dom / (double)n;
-    }
-    for (int i = 0; i < n; i++) tot += area[i];
-    if (!(tot > 0)) return fail(h, COT_EINVAL, "cot_source_masses: zero total area", nullptr);
-    for (int i = 0; i < n; i++) nu_out[i] = area[i] / tot * dom;
+    for (int i = 0; i < n; i++) tot += val[i];
+    if (!(tot > 0)) return fail(h, COT_EINVAL, "cot_source_masses: zero total", nullptr);
+    for (int i = 0; i < n; i++) nu_out[i] = val[i] / tot * dom;
     return COT_OK;
+}
+
+extern "C" int cot_source_masses(cot_handle *h, const double *points_xy, int n, const double sample_domain[4],
+                                 double *nu_out)
+{
+    if (!h) return COT_EINVAL;
+    if (!points_xy || n <= 0 || !sample_domain || !nu_out) return fail(h, COT_EINVAL, "cot_source_masses: bad argument", nullptr);
+    const double *sd = sample_domain;
+    if (!(sd[1] > sd[0]) || !(sd[3] > sd[2])) return fail(h, COT_EINVAL, "cot_source_masses: empty sample_domain", nullptr);
+    return source_masses_impl(h, points_xy, n, sd, nullptr, 0.0, nu_out);
+}
+
+extern "C" int cot_source_masses_point_light(cot_handle *h, const double *points_xy, int n,
+                                             const double sample_domain[4], const double light[3], double z_of_len,
+                                             double *nu_out)
+{
+    if (!h) return COT_EINVAL;
+    if (!points_xy || n <= 0 || !sample_domain || !light || !nu_out)
+        return fail(h, COT_EINVAL, "cot_source_masses_point_light: bad argument", nullptr);
+    const double *sd = sample_domain;
+    if (!(sd[1] > sd[0]) || !(sd[3] > sd[2])) return fail(h, COT_EINVAL, "cot_source_masses_point_light: empty sample_domain", nullptr);
+    return source_masses_impl(h, points_xy, n, sd, light, z_of_len, nu_out);
 }
 
 extern "C" int cot_render(cot_handle *h, const double *w, double gray_multiple, double *out)

@@ -647,6 +647,39 @@ __device__ __noinline__ CellAcc integrate_cell(SP &P, int nv, const PixGeo g, do
     return acc;
 }
 
+// compute_solid_angle (basic_function.cuh:558-588): solid angle of the planar
+// polygon (absolute vertices, plane z) seen from the light, as the sum over
+// the fan from vertex 0 of 2 atan(num / den), triangles with |den| < 1e-6
+// skipped, absolute value at the end.  One lane does the sum in ring order.
+template <class SP>
+__device__ double solid_angle_of(const SP &P, int nv, double2 si, double z, const double *L)
+{
+    auto unit = [](double v[3]) {
+        double l = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        v[0] /= l;
+        v[1] /= l;
+        v[2] /= l;
+    };
+    double ang = 0.0;
+    for (int k = 0; k < nv - 2; k++) {
+        double v1[3] = {si.x + P.X[0] - L[0], si.y + P.Y[0] - L[1], z - L[2]};
+        double v2[3] = {si.x + P.X[k + 1] - L[0], si.y + P.Y[k + 1] - L[1], z - L[2]};
+        double v3[3] = {si.x + P.X[k + 2] - L[0], si.y + P.Y[k + 2] - L[1], z - L[2]};
+        unit(v1);
+        unit(v2);
+        unit(v3);
+        double cr[3] = {v2[1] * v3[2] - v2[2] * v3[1], v2[2] * v3[0] - v2[0] * v3[2], v2[0] * v3[1] - v2[1] * v3[0]};
+        double num = v1[0] * cr[0] + v1[1] * cr[1] + v1[2] * cr[2];
+        double d12 = v1[0] * v2[0] + v1[1] * v2[1] + v1[2] * v2[2];
+        double d23 = v2[0] * v3[0] + v2[1] * v3[1] + v2[2] * v3[2];
+        double d13 = v1[0] * v3[0] + v1[1] * v3[1] + v1[2] * v3[2];
+        double den = 1.0 + d12 + d23 + d13;
+        if (fabs(den) < 1e-6) continue;
+        ang += 2.0 * atan(num / den);
+    }
+    return fabs(ang);
+}
+
 // Plain area centroid of the polygon (relative to the site).
 template <class SP>
 __device__ void poly_centroid(const SP &P, int nv, int lane, double &cx, double &cy)
@@ -1093,6 +1126,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
             a.ring_xy[2 * ((size_t)i * a.ring_cap + lane) + 1] = si.y + P.y;
             a.ring_lab[(size_t)i * a.ring_cap + lane] = P.l;
         }
+        if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(S, nv, si, a.solid_z, a.solid_light) : 0.0;
         if (a.nbn != nullptr) {
             // neighbours of this evaluation seed the next one
             const bool isn = lane < nv && P.l >= 0;
@@ -1341,6 +1375,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
                 a.ring_lab[(size_t)i * a.ring_cap + k] = P.L[k];
             }
         }
+        if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(P, nv, si, a.solid_z, a.solid_light) : 0.0;
         if (a.nbn != nullptr) {
             // neighbours of this evaluation seed the next one
             int lab = -1;

@@ -135,6 +135,9 @@ struct CellsArgs {
     double *cen;           // centroids (nullable)
     unsigned char *exist;  // exist flags (nullable)
     int weighted;          // centroid flavour
+    double *solid;         // solid angle of each cell from a point light (nullable)
+    double solid_z;        // plane of the cells
+    double solid_light[3]; // light position
     double *splat;         // render output, nx*ny (nullable)
     double splat_scale;    // gray_multiple of the render
     double *ring_xy;       // optional fixed-stride ring dump (nullable)

@@ -195,6 +195,15 @@ COT_API int cot_centroids(cot_handle *h, const double *w, double *xy, unsigned c
 COT_API int cot_source_masses(cot_handle *h, const double *points_xy, int n,
                       const double sample_domain[4], double *nu_out);
 
+/* Source masses of a point light at light[3]: solid angle each unweighted
+ * source cell (inside sample_domain, in the plane z_of_len) subtends from the
+ * light, normalised to total area_scalar.  Replaces solid_angle /
+ * len_solid_angle + the normalisation (basic_function.cuh:558-588,635-658;
+ * ot_op.cuh:160-206). */
+COT_API int cot_source_masses_point_light(cot_handle *h, const double *points_xy, int n,
+                                          const double sample_domain[4], const double light[3],
+                                          double z_of_len, double *nu_out);
+
 /* Diagnostic splat of nu over the pixels, nu_i * area(cell_i ∩ pixel) /
  * area(cell_i) (render, basic_function.cuh:660-741), scaled by the
  * reference's gray_multiple = sum(raw density) / area_scalar

@@ -279,6 +279,50 @@ def source_masses(points, sample_domain):
     return a / a.sum() * (xs * ys)
 
 
+def solid_angle(poly, z, light):
+    """compute_solid_angle (basic_function.cuh:558-588) of one ring."""
+    L = _f64(light)
+    P = np.column_stack([_f64(poly).reshape(-1, 2), np.full(len(poly), float(z))]) - L
+    n = len(P)
+    ang = 0.0
+    for k in range(n - 2):
+        v1 = P[0] / np.linalg.norm(P[0])
+        v2 = P[k + 1] / np.linalg.norm(P[k + 1])
+        v3 = P[k + 2] / np.linalg.norm(P[k + 2])
+        num = float(v1 @ np.cross(v2, v3))
+        den = 1.0 + float(v1 @ v2) + float(v2 @ v3) + float(v1 @ v3)
+        if abs(den) < 1e-6:
+            continue
+        ang += 2 * np.arctan(num / den)
+    return abs(ang)
+
+
+def source_masses_point_light(points, sample_domain, light, z_of_len):
+    """Point-light source masses (ot_op.cuh:160-206): solid angle of each
+    source cell clipped to the sample domain, normalised to area_scalar."""
+    L = lib()
+    sd = _f64(sample_domain)
+    xs, ys = sd[1] - sd[0], sd[3] - sd[2]
+    corner = np.array([sd[0] - xs / 40, sd[1] + xs / 40, sd[2] - ys / 40, sd[3] + ys / 40])
+    n = _f64(points).reshape(-1, 2).shape[0]
+    c = cells(points, np.zeros(n), corner)
+    sq = np.array([sd[0], sd[2], sd[1], sd[3]])
+    out = np.zeros(2 * ORC_MAXD_PY)
+    nn = ctypes.c_int()
+    om = np.zeros(n)
+    for i in range(n):
+        m = int(c.ring_len[i])
+        if m <= 0:
+            continue
+        ring = _f64(c.ring_xy[i, :m]).reshape(-1)
+        L.orc_clip_rect(_d(ring), m, _d(sq), _d(out), ctypes.byref(nn))
+        om[i] = solid_angle(out[: 2 * nn.value].reshape(-1, 2), z_of_len, light)
+    return om / om.sum() * (xs * ys)
+
+
+ORC_MAXD_PY = 512
+
+
 # --------------------------------------------------------------------------
 # evaluation bundle
 # --------------------------------------------------------------------------

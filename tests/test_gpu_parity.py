@@ -193,6 +193,20 @@ def test_source_masses_parity(gpu):
     assert np.abs(nu - onu).max() < 1e-10 * onu.max()
 
 
+def test_point_light_source_masses_parity(gpu):
+    """solid_angle (basic_function.cuh:558-588,635-658) source masses."""
+    pts = seeds.initial_xy_point(400, [0.0, 40.0, 0.0, 40.0])
+    light = [20.0, 20.0, -20.0]
+    s = capi.Solver()
+    nu = s.source_masses(pts, [0.0, 40.0, 0.0, 40.0], light=light, z_of_len=0.0)
+    onu = O.source_masses_point_light(pts, [0.0, 40.0, 0.0, 40.0], light, 0.0)
+    assert abs(nu.sum() - 1600.0) < 1e-9
+    assert np.abs(nu - onu).max() < MU_TOL * onu.max()
+    # cells right under the light see more of it than those in the corners
+    c = np.argmin(np.hypot(pts[:, 0] - 20, pts[:, 1] - 20))
+    assert nu[c] > nu[0]
+
+
 def test_torch_device_buffers(gpu):
     import torch
 
