@@ -148,7 +148,7 @@ extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
     cot_handle *h = new (std::nothrow) cot_handle();
     if (!h) return fail(nullptr, COT_ENOMEM, "cot_create: out of host memory", nullptr);
     if (cfg) h->cfg = *cfg;
-    if (h->cfg.bucket_size <= 0) h->cfg.bucket_size = 4;
+    if (h->cfg.bucket_size <= 0) h->cfg.bucket_size = 16;
     if (h->cfg.warps_per_block <= 0) h->cfg.warps_per_block = 4;
     if (h->cfg.warps_per_block > 8) h->cfg.warps_per_block = 8;
     if (h->cfg.max_ring <= 0) h->cfg.max_ring = 200;

@@ -680,6 +680,175 @@ __device__ double solid_angle_of(const SP &P, int nv, double2 si, double z, cons
     return fabs(ang);
 }
 
+// Mass and second moment of the cell, regrouped by Green's theorem.
+// For each pixel p, int over cell ∩ p of g equals the sum over the boundary
+// of cell ∩ p of G dy (dG/dx = g).  Summed over the pixels with their
+// densities this is: (a) the cell's edges, cut at the pixel lines they
+// cross, each piece weighted by its own pixel's density; plus (b) the
+// vertical pixel lines inside the cell, each segment weighted by the density
+// of the pixel on its left minus the one on its right (horizontal pieces have
+// dy = 0).  (b) also produces the fully covered pixels.  Work is O(pixels)
+// with O(1) each plus O(edge length) per edge -- no per-pixel loop over the
+// edges.  Coordinates are taken relative to the centre of the cell's box for
+// accuracy and shifted to the site at the end.  Used when neither centroids
+// (whose reference rule needs per-pixel areas) nor the render are wanted.
+template <class SP>
+__device__ __noinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, double2 si, int lane)
+{
+    CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
+    for (int k = lane; k < nv; k += 32) {
+        int kn = (k + 1 == nv) ? 0 : k + 1;
+        double dx = P.X[kn] - P.X[k], dy = P.Y[kn] - P.Y[k];
+        P.EIX[k] = dx != 0.0 ? 1.0 / dx : 0.0;
+        P.EIY[k] = dy != 0.0 ? 1.0 / dy : 0.0;
+        P.ESL[k] = dx != 0.0 ? dy / dx : 0.0;
+        mnx = fmin(mnx, P.X[k]); mxx = fmax(mxx, P.X[k]);
+        mny = fmin(mny, P.Y[k]); mxy = fmax(mxy, P.Y[k]);
+    }
+    mnx = warp_min(mnx); mxx = warp_max(mxx); mny = warp_min(mny); mxy = warp_max(mxy);
+    __syncwarp();
+    const double ox = 0.5 * (mnx + mxx), oy = 0.5 * (mny + mxy);  // local origin
+    const double cx0 = g.pd0 - si.x, cy0 = g.pd2 - si.y;           // pixel line 0, site frame
+    double sA = 0.0, sIa = 0.0, sIb = 0.0, sI2 = 0.0;
+    // (a) edge pieces, one lane per edge
+    for (int k = lane; k < nv; k += 32) {
+        int kn = (k + 1 == nv) ? 0 : k + 1;
+        const double px = P.X[k], py = P.Y[k], qx = P.X[kn], qy = P.Y[kn];
+        const double dx = qx - px, dy = qy - py;
+        if (dy == 0.0) continue;  // horizontal: no x-dy term
+        if (dx == 0.0) {
+            // a vertical edge on a pixel line is counted with the lines in (b)
+            double c = (px - cx0) * g.ixs;
+            int ci = (int)floor(c + 0.5);
+            if ((double)ci * g.xs + cx0 == px) continue;
+        }
+        const double idx = P.EIX[k], idy = P.EIY[k];
+        // crossings with vertical lines X_c and horizontal lines Y_r strictly inside
+        const int cstep = dx > 0.0 ? 1 : -1, rstep = dy > 0.0 ? 1 : -1;
+        int c = (int)floor((px - cx0) * g.ixs) + (dx > 0.0 ? 0 : 1);
+        int r = (int)floor((py - cy0) * g.iys) + (dy > 0.0 ? 0 : 1);
+        auto next_x = [&](void) -> double {
+            if (dx == 0.0) return 2.0;
+            for (int guard = 0; guard < 4; guard++) {
+                double X = (double)c * g.xs + cx0;
+                if (dx > 0.0 ? X >= qx : X <= qx) return 2.0;
+                if (dx > 0.0 ? X > px : X < px) return (X - px) * idx;
+                c += cstep;
+            }
+            return 2.0;
+        };
+        auto next_y = [&](void) -> double {
+            for (int guard = 0; guard < 4; guard++) {
+                double Y = (double)r * g.ys + cy0;
+                if (dy > 0.0 ? Y >= qy : Y <= qy) return 2.0;
+                if (dy > 0.0 ? Y > py : Y < py) return (Y - py) * idy;
+                r += rstep;
+            }
+            return 2.0;
+        };
+        double tx = next_x(), ty = next_y(), tp = 0.0;
+        for (int guard = 0; guard < 4 * (g.nx + g.ny) + 8; guard++) {
+            const double tn = fmin(fmin(tx, ty), 1.0);
+            if (tn > tp) {
+                const double ax = (tp == 0.0 ? px : px + tp * dx), ay = (tp == 0.0 ? py : py + tp * dy);
+                const double bx = (tn == 1.0 ? qx : px + tn * dx), by = (tn == 1.0 ? qy : py + tn * dy);
+                const double tm = 0.5 * (tp + tn);
+                // pixel of the piece, settled against the same line positions
+                // c * xs + x0 that the crossings and part (b) use (the
+                // product form and the quotient form can round apart at the
+                // image's far sides)
+                const double xm = px + tm * dx, ym = py + tm * dy;
+                int ix = (int)floor((xm - cx0) * g.ixs);
+                int iy = (int)floor((ym - cy0) * g.iys);
+                if ((double)ix * g.xs + cx0 > xm) ix--;
+                else if ((double)(ix + 1) * g.xs + cx0 <= xm) ix++;
+                if ((double)iy * g.ys + cy0 > ym) iy--;
+                else if ((double)(iy + 1) * g.ys + cy0 <= ym) iy++;
+                // a piece outside the image (a rounding sliver along the
+                // domain sides) carries no density
+                if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny) {
+                    if (tn >= 1.0) break;
+                    if (tn == tx) { c += cstep; tx = next_x(); }
+                    if (tn == ty) { r += rstep; ty = next_y(); }
+                    tp = tn;
+                    continue;
+                }
+                const double rho = g.rho[ix + iy * g.nx];
+                Mom m = {0.0, 0.0, 0.0, 0.0};
+                seg_terms(ax - ox, ay - oy, bx - ox, by - oy, m);
+                sA += rho * m.A;
+                sIa += rho * m.Ia;
+                sIb += rho * m.Ib;
+                sI2 += rho * m.I2;
+            }
+            if (tn >= 1.0) break;
+            if (tn == tx) { c += cstep; tx = next_x(); }
+            if (tn == ty) { r += rstep; ty = next_y(); }
+            tp = tn;
+        }
+    }
+    // (b) vertical pixel lines inside the cell
+    int lx = (int)floor((mnx - cx0) * g.ixs) - 1;
+    int ly = (int)floor((mny - cy0) * g.iys) - 1;
+    int hx = (int)floor((mxx - cx0) * g.ixs) + 2;
+    int hy = (int)floor((mxy - cy0) * g.iys) + 2;
+    lx = max(lx, 0);
+    ly = max(ly, 0);
+    hx = min(hx, g.nx);
+    hy = min(hy, g.ny);
+    for (int cxs = lx; cxs < hx; cxs += 32) {
+        const int cw = min(32, hx - cxs);
+        for (int c = lane; c <= cw; c += 32) {
+            double xl = (double)(cxs + c) * g.xs + cx0;
+            double lo, hi;
+            section_at(P, nv, xl, lo, hi);
+            P.elo[c] = lo;
+            P.ehi[c] = hi;
+            P.rv[c] = (mnx <= xl && xl < mxx) ? 1 : 0;  // right limit: left side of a pixel
+            P.lv[c] = (mnx < xl && xl <= mxx) ? 1 : 0;  // left limit: right side of a pixel
+        }
+        __syncwarp();
+        const int rows = hy - ly, npx = cw * rows;
+        for (int q = lane; q < npx; q += 32) {
+            const int c = q % cw, rr = q / cw;
+            const int ix = cxs + c, iy = ly + rr;
+            const double y0 = (double)iy * g.ys + cy0, y1 = (double)(iy + 1) * g.ys + cy0;
+            Mom m = {0.0, 0.0, 0.0, 0.0};
+            bool any = false;
+            if (P.lv[c + 1]) {  // right side of the pixel, upwards
+                double b0 = fmax(P.elo[c + 1], y0), b1 = fmin(P.ehi[c + 1], y1);
+                if (b1 > b0) {
+                    vside_terms((double)(ix + 1) * g.xs + cx0 - ox, b0 - oy, b1 - oy, m);
+                    any = true;
+                }
+            }
+            if (P.rv[c]) {      // left side, downwards
+                double b0 = fmax(P.elo[c], y0), b1 = fmin(P.ehi[c], y1);
+                if (b1 > b0) {
+                    vside_terms((double)ix * g.xs + cx0 - ox, b1 - oy, b0 - oy, m);
+                    any = true;
+                }
+            }
+            if (!any) continue;
+            const double rho = g.rho[ix + iy * g.nx];
+            sA += rho * m.A;
+            sIa += rho * m.Ia;
+            sIb += rho * m.Ib;
+            sI2 += rho * m.I2;
+        }
+        __syncwarp();
+    }
+    sA = warp_sum(sA);
+    sIa = warp_sum(sIa);
+    sIb = warp_sum(sIb);
+    sI2 = warp_sum(sI2);
+    acc.mu = sA;
+    // int |x - s_i|^2 = int |(x - o) + o|^2 in the site frame
+    acc.S = sI2 + 2.0 * (ox * sIa + oy * sIb) + (ox * ox + oy * oy) * sA;
+    return acc;
+}
+
 // Plain area centroid of the polygon (relative to the site).
 template <class SP>
 __device__ void poly_centroid(const SP &P, int nv, int lane, double &cx, double &cy)
@@ -920,7 +1089,10 @@ __device__ __noinline__ RegPoly apply_ranges(RegPoly P, int st, int cnt, int inc
     return P;
 }
 
-template <int MINB>
+// EXACT = true: the per-pixel path that also yields centroids (with the
+// reference's 1e-10 piece rule) and the render; false: the solver's hot path
+// (masses and objective only), which keeps the kernel's code small.
+template <int MINB, bool EXACT>
 __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1114,19 +1286,28 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
         if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
         __syncwarp();
         CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (nv >= 3) acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
+        if (nv >= 3) {
+            if constexpr (EXACT)
+                acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
+            else
+                acc = integrate_fast(S, nv, pix_geo(g), si, lane);
+        }
         PSTAT_CLOCK(t3);
         PSTAT_ADD(2, t3 - t2);
         PSTAT_ADD(8, 1);
         PSTAT_ADD(11, nv);
         double pcx = 0.0, pcy = 0.0;
-        if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid(S, nv, lane, pcx, pcy);
+        if constexpr (EXACT) {
+            if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid(S, nv, lane, pcx, pcy);
+        }
         if (a.ring_xy != nullptr && lane < nv && lane < a.ring_cap) {
             a.ring_xy[2 * ((size_t)i * a.ring_cap + lane)] = si.x + P.x;
             a.ring_xy[2 * ((size_t)i * a.ring_cap + lane) + 1] = si.y + P.y;
             a.ring_lab[(size_t)i * a.ring_cap + lane] = P.l;
         }
-        if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(S, nv, si, a.solid_z, a.solid_light) : 0.0;
+        if constexpr (EXACT) {
+            if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(S, nv, si, a.solid_z, a.solid_light) : 0.0;
+        }
         if (a.nbn != nullptr) {
             // neighbours of this evaluation seed the next one
             const bool isn = lane < nv && P.l >= 0;
@@ -1449,7 +1630,10 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int n
     size_t sm = sizeof(FastScratch) * CELLS_WPB;
     bool timed = c.profile && c.ev != nullptr && c.ev_used + 2 <= c.ev_cap;
     if (timed) cudaEventRecord(c.ev[c.ev_used], s);
-    k_cells_fast<CELLS_MINB><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a);
+    if (a.cen != nullptr || a.splat != nullptr || a.solid != nullptr)
+        k_cells_fast<CELLS_MINB, true><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a);
+    else
+        k_cells_fast<CELLS_MINB, false><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a);
     if (timed) {
         cudaEventRecord(c.ev[c.ev_used + 1], s);
         c.ev_used += 2;
@@ -1476,11 +1660,13 @@ extern "C" __attribute__((visibility("default"))) int cot_debug_phase_stats(unsi
 
 void configure_cells_kernels()
 {
-    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(FastScratch) * CELLS_WPB));
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(sizeof(FastScratch) * CELLS_WPB));
     cudaFuncSetAttribute(k_cells<256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(256, 1));
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB>, 32 * CELLS_WPB,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false>, 32 * CELLS_WPB,
                                                       sizeof(FastScratch) * CELLS_WPB) == cudaSuccess && nb > 0)
         g_cells_blocks_per_sm = nb;
 }

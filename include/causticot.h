@@ -72,7 +72,7 @@ typedef struct cot_handle cot_handle;
 
 typedef struct {
     int device;          /* CUDA device ordinal */
-    int bucket_size;     /* target sites per neighbour bucket (0: default 4) */
+    int bucket_size;     /* target sites per neighbour bucket (0: default 16) */
     int warps_per_block; /* cell kernel launch shape (0: default) */
     int max_ring;        /* ring-complexity reject threshold (0: 200, as
                             ot_op.cuh:376 max_edge_num/2) */
