@@ -25,6 +25,11 @@ COT_ERING = -5
 COT_ENOTCONV = -6
 COT_ETIMEOUT = -7
 COT_ENOMEM = -8
+COT_ECANCELLED = -9
+
+PHASE_LBFGS = 0
+PHASE_PREPASS = 1
+PHASE_ANDERSON = 2
 
 COT_MEM_HOST = 0
 COT_MEM_DEVICE = 1
@@ -36,7 +41,13 @@ EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
     "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_source_masses_point_light", "cot_last_error",
+    "cot_set_progress",
 ]
+# int (*)(void *user, int phase, int iteration, int status, const double *w, const double *nu, int n,
+#         double grad_norm, double max_rel_err)
+PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                               ctypes.c_double, ctypes.c_double)
 NOALLOC_MAX_N = 2048 * 1024
 
 
@@ -108,6 +119,7 @@ def load():
         L.cot_solve_aarl.argtypes = [vp, vp, ctypes.POINTER(cot_aarl_inputs), ctypes.POINTER(cot_solve_opts),
                                      ctypes.POINTER(cot_solve_stats)]
         L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+        L.cot_set_progress.argtypes = [vp, PROGRESS_FN, vp, ctypes.c_int]
         for name in EXPORTED:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -166,6 +178,39 @@ class Solver:
         self._h = h
         self.n = 0
         self.device = device
+        self._progress = None       # keeps the ctypes callback alive
+        self._progress_exc = None   # exception raised inside the callback
+
+    def set_progress(self, fn=None, every: int = 1):
+        """Call fn(phase, iteration, status, w, nu, grad_norm, max_rel_err)
+        after every iteration whose 0-based index is a multiple of `every`
+        and after the last one of each phase (status 0 running, 1 converged,
+        2 stopped; w, nu: numpy copies in caller order).  A truthy return
+        stops the solve, which then returns its last iterate with
+        converged=False.  fn may call eval / cells / centroids / render on
+        this solver.  fn=None removes the callback."""
+        if fn is None:
+            self._check(self._L.cot_set_progress(self._h, PROGRESS_FN(), None, 1))
+            self._progress = None
+            return
+
+        def tramp(user, phase, iteration, status, w, nu, n, gnorm, maxrel):
+            try:
+                wa = np.ctypeslib.as_array(w, shape=(n,)).copy()
+                na = np.ctypeslib.as_array(nu, shape=(n,)).copy()
+                return 1 if fn(phase, iteration, status, wa, na, gnorm, maxrel) else 0
+            except BaseException as e:  # stop the solve, re-raise after it returns
+                self._progress_exc = e
+                return 1
+
+        cb = PROGRESS_FN(tramp)
+        self._check(self._L.cot_set_progress(self._h, cb, None, int(every)))
+        self._progress = cb
+
+    def _raise_progress_exc(self):
+        e, self._progress_exc = self._progress_exc, None
+        if e is not None:
+            raise e
 
     def _err(self, h="self"):
         buf = ctypes.create_string_buffer(1024)
@@ -265,7 +310,8 @@ class Solver:
         else:
             w = _f64(w0).copy()
             rc = self._L.cot_solve(self._h, _vptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_HOST)
-        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV,))
+        self._raise_progress_exc()
+        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV, COT_ECANCELLED))
         stats = SolveStats(st.iterations, st.evaluations, st.restarts, bool(st.converged), st.f, st.max_rel_err,
                            st.grad_norm, st.empty_cells, st.ring_overflows, st.ms)
         return w, stats
@@ -286,7 +332,8 @@ class Solver:
         opts = cot_solve_opts(SOLVE_REFERENCE, history, max_iter, tol, initial_step, 0.0, 0.0, 0, 0)
         st = cot_solve_stats()
         rc = self._L.cot_solve_aarl(self._h, _vptr(w), ctypes.byref(ai), ctypes.byref(opts), ctypes.byref(st))
-        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV,))
+        self._raise_progress_exc()
+        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV, COT_ECANCELLED))
         return w, SolveStats(st.iterations, st.evaluations, st.restarts, bool(st.converged), st.f, st.max_rel_err,
                              st.grad_norm, st.empty_cells, st.ring_overflows, st.ms)
 

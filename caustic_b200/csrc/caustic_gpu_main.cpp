@@ -156,6 +156,63 @@ static void write_weights_file(const std::vector<double> &w, const std::string &
     for (double v : w) f << v << std::endl;
 }
 
+// Diagnostics written during a solve through the progress callback, on the
+// reference's schedule and names:
+//   starting points (iteration -1): render_initial + mesh_initial.obj of
+//     direct_ot (ot_op.cuh:214-219, 285-286); pre_render_initial +
+//     pre_initial_mesh.obj at the re-weighted warm start and render_initial
+//     after the pre-pass of aarl_direct_ot (ot_op.cuh:797-820, 1094-1099);
+//   direct_ot (ot_op.cuh:478-535): every 500 iterations weights_<it> and
+//     render_<it>; on convergence weights_, mesh_<it>.obj and render_;
+//   pre-pass of aarl_direct_ot (ot_op.cuh:1014-1074): the same with "pre_";
+//   Anderson loop (ot_op.cuh:1270-1321): <t>_weights_<it> every 200,
+//     <t>_render_<it> every 500, and all three on convergence.
+struct Diagnostics {
+    cot_handle *h = nullptr;
+    double gray = 1.0;
+    int pm = 0, pn = 0;
+    std::string render_dir, mesh_dir, wdir, ot_time;
+};
+
+static int on_progress(void *user, int phase, int iteration, int status, const double *w, const double *nu, int n,
+                       double grad_norm, double max_rel_err)
+{
+    (void)nu;
+    Diagnostics &D = *static_cast<Diagnostics *>(user);
+    const std::vector<double> wv(w, w + n);
+    if (iteration < 0) {
+        bool ok = true;
+        if (phase == COT_PHASE_LBFGS)
+            ok = write_render(D.h, wv, D.gray, D.pm, D.pn, D.render_dir + "render_initial.txt") &&
+                 write_obj(D.h, wv, D.mesh_dir + "mesh_initial.obj");
+        else if (phase == COT_PHASE_PREPASS)
+            ok = write_render(D.h, wv, D.gray, D.pm, D.pn, D.render_dir + "pre_render_initial.txt") &&
+                 write_obj(D.h, wv, D.mesh_dir + "pre_initial_mesh.obj");
+        else
+            ok = write_render(D.h, wv, D.gray, D.pm, D.pn, D.render_dir + "render_initial.txt");
+        if (!ok) std::cerr << "could not write the initial diagnostics" << std::endl;
+        return 0;
+    }
+    const std::string it = std::to_string(iteration);
+    std::string tag;
+    int weights_every = 500;
+    if (phase == COT_PHASE_PREPASS) tag = "pre_";
+    if (phase == COT_PHASE_ANDERSON) {
+        tag = D.ot_time + "_";
+        weights_every = 200;
+    }
+    if (iteration % 100 == 0 || status != 0)
+        std::cout << (phase == COT_PHASE_ANDERSON ? "aa " : phase == COT_PHASE_PREPASS ? "pre " : "") << iteration
+                  << ": |g| " << grad_norm << ", max rel " << max_rel_err << std::endl;
+    bool ok = true;
+    if (iteration % weights_every == 0 || status == 1) write_weights_file(wv, D.wdir + tag + "weights_" + it + ".txt");
+    if (iteration % 500 == 0 || status == 1)
+        ok = write_render(D.h, wv, D.gray, D.pm, D.pn, D.render_dir + tag + "render_" + it + ".txt");
+    if (status == 1) ok = write_obj(D.h, wv, D.mesh_dir + tag + "mesh_" + it + ".obj") && ok;
+    if (!ok) std::cerr << "could not write the diagnostics of iteration " << iteration << std::endl;
+    return 0;
+}
+
 static int solver_error(cot_handle *h, const char *what)
 {
     char buf[512];
@@ -313,7 +370,7 @@ int main(int argc, char *argv[])
     if (cot_set_problem(h, proj_xy.data(), nu.data(), n, picture.data(), pm, pn, proj_domain.data(), COT_MEM_HOST) != COT_OK)
         return solver_error(h, "cot_set_problem");
 
-    // diagnostics of the reference (ot_op.cuh:214-219, 281-286): the starting cells
+    // diagnostics of the reference, written from the solve's progress reports
     double raw_sum = 0;
     for (double v : picture) raw_sum += v;
     const double area_scalar = (sample_domain[1] - sample_domain[0]) * (sample_domain[3] - sample_domain[2]);
@@ -321,10 +378,17 @@ int main(int argc, char *argv[])
     const std::string render_dir = "../render_result/" + xiushi + "/" + ot_time + "/";
     const std::string mesh_dir = "../mesh_output/" + xiushi + "/" + ot_time + "/";
     const std::string wdir = "../weights/" + xiushi + "/" + ot_time + "/";
-    const std::string pre = ot_time == "0" ? "" : "pre_";
-    if (!write_render(h, w, gray, pm, pn, render_dir + pre + "render_initial.txt") ||
-        !write_obj(h, w, mesh_dir + (ot_time == "0" ? "mesh_initial.obj" : "pre_initial_mesh.obj")))
-        std::cerr << "could not write the initial diagnostics" << std::endl;
+
+    Diagnostics diag;
+    diag.h = h;
+    diag.gray = gray;
+    diag.pm = pm;
+    diag.pn = pn;
+    diag.render_dir = render_dir;
+    diag.mesh_dir = mesh_dir;
+    diag.wdir = wdir;
+    diag.ot_time = ot_time;
+    if (cot_set_progress(h, on_progress, &diag, 100) != COT_OK) return solver_error(h, "cot_set_progress");
 
     cot_solve_opts o{};
     o.mode = COT_SOLVE_REFERENCE;
@@ -357,15 +421,6 @@ int main(int argc, char *argv[])
     if (rc != COT_OK && rc != COT_ENOTCONV) return solver_error(h, "solve");
     std::cout << "iterations " << st.iterations << ", evaluations " << st.evaluations << ", |g| " << st.grad_norm
               << ", max rel " << st.max_rel_err << ", converged " << st.converged << ", " << st.ms << " ms" << std::endl;
-    // diagnostics at the end (ot_op.cuh:510-535, 1296-1321)
-    {
-        const std::string tag = (ot_time == "0" ? "" : ot_time + "_") + std::string("");
-        const std::string it = std::to_string(st.iterations > 0 ? st.iterations - 1 : 0);
-        write_weights_file(w, wdir + tag + "weights_" + it + ".txt");
-        if (!write_obj(h, w, mesh_dir + tag + "mesh_" + it + ".obj") ||
-            !write_render(h, w, gray, pm, pn, render_dir + tag + "render_" + it + ".txt"))
-            std::cerr << "could not write the final diagnostics" << std::endl;
-    }
     std::vector<double> cen(2 * (size_t)n);
     std::vector<unsigned char> ex(n);
     if (cot_centroids(h, w.data(), cen.data(), ex.data(), 1, COT_MEM_HOST) != COT_OK) return solver_error(h, "cot_centroids");

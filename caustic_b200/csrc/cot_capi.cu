@@ -33,9 +33,11 @@ struct CotProblemDev {
     CotGeo geo{};
     // per evaluation
     double *w = nullptr, *wt = nullptr, *d = nullptr, *mu = nullptr, *mut = nullptr, *fc = nullptr;
+    double *wq = nullptr;  // weights of the query entry points, apart from a solve's iterate w
     double *phibar = nullptr;
     int *nv = nullptr, *ovf_list = nullptr, *ovf_count = nullptr;
-    int *nbc = nullptr, *nbn = nullptr;
+    int *nbc = nullptr, *nbn = nullptr;        // neighbour cache of the solves
+    int *nbc_q = nullptr, *nbn_q = nullptr;    // and of the query entry points
     double *partials = nullptr;
     unsigned int *ticket = nullptr;
     CotEvalOut *out = nullptr;
@@ -57,6 +59,11 @@ struct cot_handle {
     bool has_problem = false;
     CotSolver *hS = nullptr;  // pinned mirror of the control block
     cot::CotCtx ctx;
+    // progress callback (cot_set_progress) and its caller-order buffers
+    cot_progress_fn prog_fn = nullptr;
+    void *prog_user = nullptr;
+    int prog_every = 1;
+    std::vector<double> prog_w, prog_nu;
     cot::CotCtx &c()
     {
         ctx.s = stream;
@@ -126,7 +133,7 @@ using namespace cot;
 static void free_problem(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
-                    P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_count, P.nbc, P.nbn, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
+                    P.wq, P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
                     P.Yv};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -210,6 +217,16 @@ extern "C" int cot_set_stream(cot_handle *h, void *s)
 {
     if (!h) return COT_EINVAL;
     h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return COT_OK;
+}
+
+extern "C" int cot_set_progress(cot_handle *h, cot_progress_fn fn, void *user, int every)
+{
+    if (!h) return COT_EINVAL;
+    if (fn && every < 1) return fail(h, COT_EINVAL, "cot_set_progress: every must be >= 1", nullptr);
+    h->prog_fn = fn;
+    h->prog_user = fn ? user : nullptr;
+    h->prog_every = fn ? every : 1;
     return COT_OK;
 }
 
@@ -393,6 +410,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.perm, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.w, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.wt, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.wq, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.d, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mu, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mut, N * 8);
@@ -403,6 +421,8 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.ovf_count, 4 * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbc, N * COT_NBC * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbn, N * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.nbn_q, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.partials, (size_t)reduce_blocks(n) * (5 * COT_MAX_HIST + 8) * 8);
     if (e == cudaSuccess) e = A((void **)&P.ticket, sizeof(unsigned int));
     if (e == cudaSuccess) e = A((void **)&P.out, sizeof(CotEvalOut));
@@ -422,6 +442,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 4 * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
 
     CotGeo &g = P.geo;
@@ -531,8 +552,12 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.ovf_list = P.ovf_list;
     a.ovf_count = P.ovf_count;
     a.work = P.ovf_count + 1;
-    a.nbc = P.nbc;
-    a.nbn = P.nbn;
+    // the query entry points (weights in P.wq) keep their own neighbour cache
+    // so that a query made during a solve does not change the solve's clip
+    // order
+    const bool query = (w == P.wq);
+    a.nbc = query ? P.nbc_q : P.nbc;
+    a.nbn = query ? P.nbn_q : P.nbn;
     return a;
 }
 
@@ -546,21 +571,24 @@ extern "C" int cot_eval(cot_handle *h, const double *w, double *f_total, double 
     CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
     int r;
-    if ((r = upload_sorted(h, w, mem, P.w)) != COT_OK) return r;
-    CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+    if ((r = upload_sorted(h, w, mem, P.wq)) != COT_OK) return r;
+    CellsArgs a = cells_args(P, P.wq, nullptr, nullptr);
     launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
     launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
     COT_CUDA_TRY(cudaGetLastError());
     CotEvalOut o;
     COT_CUDA_TRY(cudaMemcpyAsync(&o, P.out, sizeof o, cudaMemcpyDeviceToHost, s));
     if (mu && (r = download_sorted(h, P.mut, mu, mem)) != COT_OK) return r;
+    // per-cell results staged in the second half of P.tmp (the first half
+    // is the scatter's staging); the solve's vectors stay untouched
+    double *stage = P.tmp + P.n;
     if (f_cell) {
-        launch_fcell_full(P.n, P.fc, P.wt, P.nu, P.d, h->c());
-        if ((r = download_sorted(h, P.d, f_cell, mem)) != COT_OK) return r;
+        launch_fcell_full(P.n, P.fc, P.wt, P.nu, stage, h->c());
+        if ((r = download_sorted(h, stage, f_cell, mem)) != COT_OK) return r;
     }
     if (g) {
-        k_grad<<<nblk(P.n), 256, 0, s>>>(P.n, P.mut, P.nu, P.d);
-        if ((r = download_sorted(h, P.d, g, mem)) != COT_OK) return r;
+        k_grad<<<nblk(P.n), 256, 0, s>>>(P.n, P.mut, P.nu, stage);
+        if ((r = download_sorted(h, stage, g, mem)) != COT_OK) return r;
     }
     COT_CUDA_TRY(cudaStreamSynchronize(s));
     if (f_total) *f_total = o.f;
@@ -587,11 +615,11 @@ extern "C" int cot_cells(cot_handle *h, const double *w, int *ring_offsets, doub
         cudaFree(rxy);
         return fail(h, COT_ENOMEM, "cot_cells: device allocation", cudaGetErrorString(e));
     }
-    int r = upload_sorted(h, w, COT_MEM_HOST, P.w);
+    int r = upload_sorted(h, w, COT_MEM_HOST, P.wq);
     std::vector<double> hxy;
     std::vector<int> hlab, hnv(N);
     if (r == COT_OK) {
-        CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+        CellsArgs a = cells_args(P, P.wq, nullptr, nullptr);
         a.ring_xy = rxy;
         a.ring_lab = rlab;
         a.ring_cap = cap;
@@ -643,7 +671,7 @@ extern "C" int cot_centroids(cot_handle *h, const double *w, double *xy, unsigne
     cudaStream_t s = h->stream;
     size_t N = (size_t)P.n;
     int r;
-    if ((r = upload_sorted(h, w, mem, P.w)) != COT_OK) return r;
+    if ((r = upload_sorted(h, w, mem, P.wq)) != COT_OK) return r;
     double *cen = nullptr;
     unsigned char *ex = nullptr, *ex2 = nullptr;
     COT_CUDA_TRY(cudaMalloc(&cen, N * 2 * 8 * 2));
@@ -653,7 +681,7 @@ extern "C" int cot_centroids(cot_handle *h, const double *w, double *xy, unsigne
         return fail(h, COT_ENOMEM, "cot_centroids: device allocation", cudaGetErrorString(e));
     }
     ex2 = ex + N;
-    CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+    CellsArgs a = cells_args(P, P.wq, nullptr, nullptr);
     a.cen = cen;
     a.exist = ex;
     a.weighted = weighted ? 1 : 0;
@@ -749,10 +777,10 @@ extern "C" int cot_render(cot_handle *h, const double *w, double gray_multiple, 
     const size_t npx = (size_t)P.geo.nx * P.geo.ny;
     double *img = nullptr;
     COT_CUDA_TRY(cudaMalloc(&img, npx * 8));
-    int r = upload_sorted(h, w, COT_MEM_HOST, P.w);
+    int r = upload_sorted(h, w, COT_MEM_HOST, P.wq);
     cudaError_t e = cudaMemsetAsync(img, 0, npx * 8, s);
     if (r == COT_OK && e == cudaSuccess) {
-        CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+        CellsArgs a = cells_args(P, P.wq, nullptr, nullptr);
         a.splat = img;
         a.splat_scale = gray_multiple;
         launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
@@ -783,7 +811,28 @@ static int check_opts(cot_handle *h, cot_solve_opts &o)
 
 // Device L-BFGS from the weights in P.w (sorted order).  On return P.w holds
 // the last accepted point, P.mu its masses, and *out the control block.
-static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms)
+// Progress report: the solve's iterate (sorted w on the device) and the
+// masses in force, in caller order, handed to the callback.  Returns
+// COT_ECANCELLED when the callback asks to stop.
+static int report_progress(cot_handle *h, int phase, int iteration, int status, double grad_norm,
+                           double max_rel_err)
+{
+    CotProblemDev &P = h->P;
+    h->prog_w.resize(P.n);
+    h->prog_nu.resize(P.n);
+    int r;
+    if ((r = download_sorted(h, P.w, h->prog_w.data(), COT_MEM_HOST)) != COT_OK) return r;
+    COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if ((r = download_sorted(h, P.nu, h->prog_nu.data(), COT_MEM_HOST)) != COT_OK) return r;
+    COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->prog_fn(h->prog_user, phase, iteration, status, h->prog_w.data(), h->prog_nu.data(), P.n, grad_norm,
+                   max_rel_err))
+        return failf(h, COT_ECANCELLED, "solve stopped by the progress callback after iteration %d", iteration);
+    return COT_OK;
+}
+
+static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms, int phase,
+                        bool report_start)
 {
     CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
@@ -828,13 +877,47 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
         launch_init_from_eval(P.S, P.out, h->c());
         launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, h->c());
     }
+    if (h->prog_fn && report_start) {
+        // the starting point (iteration -1)
+        COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
+        COT_CUDA_TRY(cudaStreamSynchronize(s));
+        const CotSolver snap = hs;
+        int r = report_progress(h, phase, -1, 0, std::sqrt(snap.gnorm2), snap.maxrel);
+        hs = snap;
+        if (r != COT_OK) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            out = hs;
+            if (ms) *ms = 0.0f;
+            return r;
+        }
+    }
     const size_t ctl = 16 * sizeof(int);
+    int reported = 0;
     double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
     while (true) {
         launch_begin_iteration(P.S, h->c());
         launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, h->c());
         COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
         COT_CUDA_TRY(cudaStreamSynchronize(s));
+        if (h->prog_fn && hs.iter > 0 && hs.iter != reported && ((hs.iter - 1) % h->prog_every == 0 || hs.done)) {
+            // iteration hs.iter - 1 is complete; the whole control block
+            // carries its |g| and max-rel figures
+            reported = hs.iter;
+            COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
+            COT_CUDA_TRY(cudaStreamSynchronize(s));
+            const CotSolver snap = hs;
+            const int status = !snap.done ? 0 : (snap.converged ? 1 : 2);
+            int r = report_progress(h, phase, snap.iter - 1, status, std::sqrt(snap.gnorm2), snap.maxrel);
+            hs = snap;
+            if (r != COT_OK) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                out = hs;
+                if (ms) *ms = 0.0f;
+                return r;
+            }
+        }
         if (hs.done) break;
         while (true) {
             CellsArgs a = cells_args(P, P.w, P.d, tptr);
@@ -889,7 +972,15 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
     if ((r = upload_sorted(h, w_inout, mem, h->P.w)) != COT_OK) return r;
     CotSolver hs;
     float ms = 0;
-    if ((r = solve_device(h, o, hs, &ms)) != COT_OK) return r;
+    const int rs = solve_device(h, o, hs, &ms, COT_PHASE_LBFGS, true);
+    if (rs == COT_ECANCELLED) {
+        // the last iterate goes back to the caller
+        if ((r = download_sorted(h, h->P.w, w_inout, mem)) != COT_OK) return r;
+        COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        fill_stats(hs, ms, stats);
+        return rs;
+    }
+    if (rs != COT_OK) return rs;
     if ((r = download_sorted(h, h->P.w, w_inout, mem)) != COT_OK) return r;
     COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
     fill_stats(hs, ms, stats);
@@ -1039,20 +1130,46 @@ extern "C" int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inp
     };
     // 1. nu from the centroids at the warm start
     if (eval_with_nu(nullptr, nullptr, true) < 0) return cuda_fail("cot_solve_aarl: first evaluation", cudaGetLastError());
+    // masses of the current point kept in P.mu: a progress callback may
+    // evaluate on the handle, which reuses the trial buffers
+    AARL_TRY(cudaMemcpyAsync(P.mu, P.mut, N * 8, cudaMemcpyDeviceToDevice, s));
+    // start of the pre-pass phase (reported whether or not the pre-pass runs)
+    auto report_start = [&](int phase) -> int {
+        if (!h->prog_fn) return COT_OK;
+        int rr = report_progress(h, phase, -1, 0, std::sqrt(ho.gnorm2), ho.maxrel);
+        if (rr != COT_OK) {
+            if (rr == COT_ECANCELLED && download_sorted(h, P.w, w_inout, COT_MEM_HOST) == COT_OK) {
+                cudaStreamSynchronize(s);
+                if (stats) *stats = cot_solve_stats{};
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            release();
+        }
+        return rr;
+    };
+    if ((r = report_start(COT_PHASE_PREPASS)) != COT_OK) return r;
     // 2. optional L-BFGS pre-pass with nu fixed (ot_op.cuh:823-1074)
     CotSolver pre{};
     if (in->lbfgs_prepass) {
         float pms = 0;
-        if ((r = solve_device(h, o, pre, &pms)) != COT_OK) {
+        if ((r = solve_device(h, o, pre, &pms, COT_PHASE_PREPASS, false)) != COT_OK) {
+            if (r == COT_ECANCELLED && download_sorted(h, P.w, w_inout, COT_MEM_HOST) == COT_OK) {
+                cudaStreamSynchronize(s);
+                fill_stats(pre, 0.0f, stats);
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
             release();
             return r;
         }
         evals += pre.evals;
         // 3. nu again from the centroids at the pre-pass result
         if (eval_with_nu(nullptr, nullptr, true) < 0) return cuda_fail("cot_solve_aarl: evaluation", cudaGetLastError());
+        AARL_TRY(cudaMemcpyAsync(P.mu, P.mut, N * 8, cudaMemcpyDeviceToDevice, s));
     }
-    // current point: P.w, masses P.mut, nu in P.nu
-    AARL_TRY(cudaMemcpyAsync(P.mu, P.mut, N * 8, cudaMemcpyDeviceToDevice, s));
+    // current point: P.w, masses P.mu, nu in P.nu
+    if ((r = report_start(COT_PHASE_ANDERSON)) != COT_OK) return r;
     double f = ho.f, gnorm = std::sqrt(ho.gnorm2), maxrel = ho.maxrel;
     int empty = ho.empty;
     // 4. Anderson acceleration on w <- w + alpha g (ot_op.cuh:1112-1323)
@@ -1110,7 +1227,32 @@ extern "C" int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inp
         // the reference counts empty cells (of the masses at the start of the
         // iteration) only on every tenth iteration (ot_op.cuh:1256-1268)
         const int check_degenerate = (it % 10 == 0) ? empty_start : 0;
-        if (gnorm < o.tol && check_degenerate == 0) {
+        const bool conv_now = gnorm < o.tol && check_degenerate == 0;
+        const bool last_it = conv_now || it + 1 == o.max_iter;
+        if (h->prog_fn && (it % h->prog_every == 0 || last_it)) {
+            const int status = conv_now ? 1 : (last_it ? 2 : 0);
+            if ((r = report_progress(h, COT_PHASE_ANDERSON, it, status, gnorm, maxrel)) != COT_OK) {
+                if (r == COT_ECANCELLED && download_sorted(h, P.w, w_inout, COT_MEM_HOST) == COT_OK) {
+                    cudaStreamSynchronize(s);
+                    if (stats) {
+                        *stats = cot_solve_stats{};
+                        stats->iterations = iters;
+                        stats->evaluations = evals;
+                        stats->restarts = restarts;
+                        stats->f = f;
+                        stats->max_rel_err = maxrel;
+                        stats->grad_norm = gnorm;
+                        stats->empty_cells = empty;
+                        stats->ring_overflows = ring_rejects;
+                    }
+                }
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                release();
+                return r;
+            }
+        }
+        if (conv_now) {
             converged = true;
             break;
         }

@@ -52,7 +52,8 @@ enum {
     COT_ERING = -5,        /* a cell exceeded the vertex capacity */
     COT_ENOTCONV = -6,     /* solver stopped before the tolerance */
     COT_ETIMEOUT = -7,     /* a bounded device wait gave up */
-    COT_ENOMEM = -8        /* allocation failed */
+    COT_ENOMEM = -8,       /* allocation failed */
+    COT_ECANCELLED = -9    /* the progress callback asked the solve to stop */
 };
 
 enum { COT_MEM_HOST = 0, COT_MEM_DEVICE = 1 };
@@ -181,6 +182,38 @@ typedef struct {
  * re-weighted ones.  w_inout in host memory. */
 COT_API int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inputs *in,
                            const cot_solve_opts *opts, cot_solve_stats *stats);
+
+/* Progress of a solve.  The phases are the reference's three loops:
+ * COT_PHASE_LBFGS (direct_ot, ot_op.cuh:289-537, i.e. cot_solve),
+ * COT_PHASE_PREPASS (the L-BFGS pre-pass of aarl_direct_ot,
+ * ot_op.cuh:823-1074) and COT_PHASE_ANDERSON (its Anderson loop,
+ * ot_op.cuh:1135-1323). */
+enum { COT_PHASE_LBFGS = 0, COT_PHASE_PREPASS = 1, COT_PHASE_ANDERSON = 2 };
+
+/* Called at the start of each phase (iteration = -1: the starting point,
+ * after the masses of that phase are set), after every iteration whose
+ * 0-based index (the reference's `iter`) is a multiple of `every`, and after
+ * the last iteration of each phase.  cot_solve_aarl reports the start of the
+ * pre-pass phase even when the pre-pass is off.
+ * status: 0 the phase goes on, 1 it has just converged, 2 it has stopped
+ * without converging (iteration limit or line-search failure).  w: the
+ * weights after that iteration; nu: the target masses in force (re-weighted
+ * ones in the Anderson phase); both host arrays of n doubles in caller order,
+ * valid during the call only.  grad_norm = ||mu - nu||_2 and max_rel_err at
+ * w.  The callback may call cot_eval, cot_cells, cot_centroids and
+ * cot_render on the same handle: those stage their weights apart from the
+ * solve's iterate and leave its state alone.  It must not call
+ * cot_set_problem or start another solve on the handle.  A non-zero return
+ * stops the solve with COT_ECANCELLED (w_inout then holds the last iterate).
+ * This is how the caustic_GPU shim writes the reference's periodic and final
+ * weights_<iter>.txt, render_<iter>.txt and mesh_<iter>.obj
+ * (ot_op.cuh:484-535, 1020-1074, 1270-1321). */
+typedef int (*cot_progress_fn)(void *user, int phase, int iteration, int status, const double *w,
+                               const double *nu, int n, double grad_norm, double max_rel_err);
+
+/* Install (fn != NULL, every >= 1) or remove (fn == NULL) the progress
+ * callback of a handle. */
+COT_API int cot_set_progress(cot_handle *h, cot_progress_fn fn, void *user, int every);
 
 /* Density-weighted (weighted=1) or plain centroids of the cells at w and
  * the exist flags.  Replaces compute_center (basic_function.cuh:1056-1191,

@@ -113,10 +113,26 @@ def test_file_contract_first_and_second_outer_iteration(gpu, cli, tmp_path):
     with open(os.path.join(ot, "mesh_output", XIUSHI, "0", "mesh_initial.obj")) as f:
         faces = [ln for ln in f if ln.startswith("f ")]
     assert len(faces) == len(pts)
-    assert any(fn.startswith("weights_") for fn in os.listdir(os.path.join(ot, "weights", XIUSHI, "0")))
+    # periodic files of iteration 0 and the files of the converged iteration
+    # (ot_op.cuh:484-535): weights_<it>, render_<it>, mesh_<it>.obj
+    wnames = os.listdir(os.path.join(ot, "weights", XIUSHI, "0"))
+    assert "weights_0.txt" in wnames
+    assert os.path.exists(os.path.join(ot, "render_result", XIUSHI, "0", "render_0.txt"))
+    last = max(int(fn[len("weights_"):-4]) for fn in wnames)
+    assert last > 0
+    assert os.path.exists(os.path.join(ot, "mesh_output", XIUSHI, "0", f"mesh_{last}.obj"))
+    assert os.path.exists(os.path.join(ot, "render_result", XIUSHI, "0", f"render_{last}.txt"))
+    wl = seeds.read_weights(os.path.join(ot, "weights", XIUSHI, "0", f"weights_{last}.txt"))
+    assert np.array_equal(wl, w)   # the converged iterate is the final one
     # second outer iteration: warm start + Fresnel-reweighted Anderson solve
     r = subprocess.run([cli, "1", XIUSHI], cwd=build_dir, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     w1 = seeds.read_weights(os.path.join(root, "data", "weights", XIUSHI, "1", "final_proj_point_weights.txt"))
     assert len(w1) == len(pts) and np.isfinite(w1).all()
     assert os.path.exists(os.path.join(root, "data", "point_data", XIUSHI, "1", "out.txt"))
+    # pre-pass files (ot_op.cuh:1020-1074) and the Anderson loop's, tagged
+    # with the outer iteration (ot_op.cuh:1270-1321)
+    wn1 = os.listdir(os.path.join(ot, "weights", XIUSHI, "1"))
+    assert "pre_weights_0.txt" in wn1 and "1_weights_0.txt" in wn1
+    assert os.path.exists(os.path.join(ot, "render_result", XIUSHI, "1", "1_render_0.txt"))
+    assert os.path.exists(os.path.join(ot, "render_result", XIUSHI, "1", "pre_render_initial.txt"))
