@@ -46,6 +46,10 @@ __shared__ unsigned long long cot_pst[8][16];
 #define PSTAT_CLOCK(var) do { } while (0)
 #endif
 #define COT_WIN 1  // window radius in buckets
+// neighbour cache count nbn[i]: +m an ordered ring of m generators, -m an
+// unordered list of m sites, -(COT_NB_HIDDEN + m) the m sites that hid the
+// cell at the last evaluation
+#define COT_NB_HIDDEN 100
 
 // ---------------------------------------------------------------------------
 // bucket and tree plane bounds (per evaluation)
@@ -216,26 +220,28 @@ __device__ __forceinline__ double warp_max(double v)
 __device__ __forceinline__ bool line_meet(double a1, double b1, double c1, double a2, double b2,
                                           double c2, double &x, double &y)
 {
+    // an axis-parallel line (a domain side) gives one coordinate directly;
+    // explicit roundings keep the other the same whichever line came first
     if (b1 == 0.0 && a1 != 0.0) {
-        x = c1 / a1;
+        x = __ddiv_rn(c1, a1);
         if (b2 == 0.0) return false;
-        y = (c2 - a2 * x) / b2;
+        y = __ddiv_rn(__dsub_rn(c2, __dmul_rn(a2, x)), b2);
         return true;
     }
     if (a1 == 0.0 && b1 != 0.0) {
-        y = c1 / b1;
+        y = __ddiv_rn(c1, b1);
         if (a2 == 0.0) return false;
-        x = (c2 - b2 * y) / a2;
+        x = __ddiv_rn(__dsub_rn(c2, __dmul_rn(b2, y)), a2);
         return true;
     }
     if (b2 == 0.0 && a2 != 0.0) {
-        x = c2 / a2;
-        y = (c1 - a1 * x) / b1;
+        x = __ddiv_rn(c2, a2);
+        y = __ddiv_rn(__dsub_rn(c1, __dmul_rn(a1, x)), b1);
         return true;
     }
     if (a2 == 0.0 && b2 != 0.0) {
-        y = c2 / b2;
-        x = (c1 - b1 * y) / a1;
+        y = __ddiv_rn(c2, b2);
+        x = __ddiv_rn(__dsub_rn(c1, __dmul_rn(b1, y)), a1);
         return true;
     }
     // uncontracted products: swapping the two lines negates numerator and
@@ -247,6 +253,29 @@ __device__ __forceinline__ bool line_meet(double a1, double b1, double c1, doubl
     x = __ddiv_rn(__dsub_rn(__dmul_rn(c1, b2), __dmul_rn(c2, b1)), det);
     y = __ddiv_rn(__dsub_rn(__dmul_rn(a1, c2), __dmul_rn(a2, c1)), det);
     return true;
+}
+
+// Half-plane of site j in the frame of site i: e.x <= (|e|^2 - (w_j - w_i))/2
+// with e = s_j - s_i.  One explicitly rounded form for every path that
+// builds a ring, so that the same pair of lines always meets in the same bits.
+__device__ __forceinline__ void site_line(double2 sj, double2 si, double wj, double wi, double &a, double &b,
+                                          double &c, double &key)
+{
+    a = __dsub_rn(sj.x, si.x);
+    b = __dsub_rn(sj.y, si.y);
+    key = __fma_rn(a, a, __dmul_rn(b, b));
+    c = __dmul_rn(0.5, __dsub_rn(key, __dsub_rn(wj, wi)));
+}
+
+// Domain side k (0 bottom, 1 right, 2 top, 3 left; generator -(k+1)) in the
+// site's frame, box = {x0, x1, y0, y1} = domain - site: the line of the
+// starting rectangle's edge k.
+__device__ __forceinline__ void side_line(int k, double4 box, double &a, double &b, double &c)
+{
+    const double x0 = box.x, x1 = box.y, y0 = box.z, y1 = box.w;
+    a = k == 1 ? 1.0 : (k == 3 ? -1.0 : 0.0);
+    b = k == 0 ? -1.0 : (k == 2 ? 1.0 : 0.0);
+    c = k == 0 ? -y0 : (k == 1 ? x1 : (k == 2 ? y1 : -x0));
 }
 
 // Shared scratch of one warp for the large-ring path (rings up to MAXV).
@@ -343,13 +372,7 @@ __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, dou
             if (P.L[k] == j) { act = false; break; }
     }
     double a = 0.0, b = 0.0, c = 0.0, key = INFINITY;
-    if (act) {
-        double2 sj = g.xy[j];
-        a = sj.x - si.x;
-        b = sj.y - si.y;
-        key = a * a + b * b;
-        c = 0.5 * (key - (wt[j] - wi));
-    }
+    if (act) site_line(g.xy[j], si, wt[j], wi, a, b, c, key);
     while (true) {
         bool cut = false;
         if (act) {
@@ -881,6 +904,8 @@ struct FastScratch {
     double elo[33], ehi[33];
     double slo[32], shi[32];
     unsigned char lv[33], rv[33];
+    int KL[32];                       // ring labels just before the ring emptied
+    int kn, kill;                     // their count and the label that emptied it
 };
 
 // Lane k < nv holds vertex k and the line a x + b y <= c (generator l) of the
@@ -906,6 +931,12 @@ __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, 
     const unsigned outm = __ballot_sync(FULLMASK, valid && d > 0.0);
     if (outm == 0u) return true;
     if (outm == vm) {
+        // hidden cell: remember what hid it, to seed the next evaluation
+        if (valid) S.KL[lane] = P.l;
+        if (lane == 0) {
+            S.kn = nv;
+            S.kill = lab;
+        }
         P.nv = 0;
         return true;
     }
@@ -1012,13 +1043,7 @@ __device__ __noinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__
 {
     if (__ballot_sync(FULLMASK, jl >= 0) == 0u) return P;
     double al = 0.0, bl = 0.0, cl = 0.0, key = INFINITY;
-    if (jl >= 0) {
-        double2 sj = sxy[jl];
-        al = sj.x - si.x;
-        bl = sj.y - si.y;
-        key = al * al + bl * bl;
-        cl = 0.5 * (key - (wt[jl] - wi));
-    }
+    if (jl >= 0) site_line(sxy[jl], si, wt[jl], wi, al, bl, cl, key);
     const int nv = P.nv;
     if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; S.L[lane] = P.l; }
     __syncwarp();
@@ -1058,6 +1083,73 @@ __device__ __noinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__
             return P;
         }
         if (P.nv != before) PSTAT_ADD(3, 1);
+    }
+    return P;
+}
+
+// The ring of the last evaluation, rebuilt in one step: lane k < m holds the
+// generator `lab` of edge k (a site, or -1..-4 for a domain side), vertex k
+// is where the lines of edges k-1 and k meet.  Accepted only if every vertex
+// lies inside every other line, every edge runs forward along its line and
+// every corner turns left; the ring is then the intersection of those
+// half-planes, with the vertices a sequence of clips would compute (same
+// line pair, same symmetric meet).  Otherwise the result has nv = -2 and
+// the caller clips.  Cuts by sites outside the list are found by the
+// certificate; cuts by domain sides outside it are applied here (nv = -1:
+// the ring grew past 32 vertices).
+__device__ __noinline__ RegPoly ring_from_cache(int lab, int m, const double2 *__restrict__ sxy, double4 box,
+                                                double2 si, double wi, const double *__restrict__ wt, int lane,
+                                                FastScratch &S)
+{
+    RegPoly P;
+    const bool act = lane < m;
+    double la = 0.0, lb = 0.0, lc = 0.0, key;
+    if (act) {
+        if (lab >= 0) site_line(sxy[lab], si, wt[lab], wi, la, lb, lc, key);
+        else side_line(-lab - 1, box, la, lb, lc);
+    }
+    const int pv = act ? (lane == 0 ? m - 1 : lane - 1) : lane;
+    const int nx = act ? (lane + 1 == m ? 0 : lane + 1) : lane;
+    const double pa = __shfl_sync(FULLMASK, la, pv), pb = __shfl_sync(FULLMASK, lb, pv);
+    const double pc = __shfl_sync(FULLMASK, lc, pv);
+    double vx = 0.0, vy = 0.0;
+    bool ok = true;
+    if (act) ok = line_meet(pa, pb, pc, la, lb, lc, vx, vy);
+    for (int j = 0; j < m; j++) {
+        const double ja = __shfl_sync(FULLMASK, la, j), jb = __shfl_sync(FULLMASK, lb, j);
+        const double jc = __shfl_sync(FULLMASK, lc, j);
+        if (act && j != lane && j != pv && side(ja, jb, jc, vx, vy) > 0.0) ok = false;
+    }
+    const double nvx = __shfl_sync(FULLMASK, vx, nx), nvy = __shfl_sync(FULLMASK, vy, nx);
+    const double na = __shfl_sync(FULLMASK, la, nx), nb = __shfl_sync(FULLMASK, lb, nx);
+    if (act) {
+        // edge k runs along (-b, a) from vertex k to vertex k+1
+        const double len = __fma_rn(nvx - vx, -lb, __dmul_rn(nvy - vy, la));
+        const double turn = __fma_rn(-lb, na, __dmul_rn(la, nb));
+        if (!(len > 0.0) || !(turn > 0.0)) ok = false;
+    }
+    if (!__all_sync(FULLMASK, ok)) {
+        P.nv = -2;
+        return P;
+    }
+    P.x = vx;
+    P.y = vy;
+    P.a = la;
+    P.b = lb;
+    P.c = lc;
+    P.l = act ? lab : 0;
+    P.nv = m;
+    // domain sides that the cell now reaches
+    for (int k = 0; k < 4 && P.nv > 0; k++) {
+        double a, b, c;
+        side_line(k, box, a, b, c);
+        const bool out = lane < P.nv && side(a, b, c, P.x, P.y) > 0.0;
+        if (__any_sync(FULLMASK, out)) {
+            if (!rclip(P, a, b, c, -(k + 1), lane, S)) {
+                P.nv = -1;
+                return P;
+            }
+        }
     }
     return P;
 }
@@ -1124,16 +1216,40 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
             P.l = -(lane + 1);
         }
         bool ok = true;
+        if (lane == 0) S.kn = -1;
+        __syncwarp();
         const int bi = g.sbucket[i];
         const int bu = bi % g.bx, bv = bi / g.bx;
-        // ---- 1. first candidates: last evaluation's neighbours, else the
-        //         3x3 buckets around the site, nearest first -------------------
-        const int ncache = (a.nbn != nullptr) ? a.nbn[i] : 0;
-        const bool cached = ncache > 0;
+        // ---- 1. first candidates: last evaluation's ring or neighbours, else
+        //         the 3x3 buckets around the site, nearest first ---------------
+        // cache: +m = the ring's m generators in order (domain sides
+        // included), -m = m sites in no order (long rings), hidden cells
+        // -(COT_NB_HIDDEN + m)
+        const int nraw = (a.nbn != nullptr) ? a.nbn[i] : 0;
+        const bool hidden = nraw < -COT_NB_HIDDEN;
+        const int ncache = min(nraw >= 0 ? nraw : (hidden ? -nraw - COT_NB_HIDDEN : -nraw), COT_NBC);
+        bool cached = ncache > 0;
         if (cached) {
-            int j = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
-            P = apply_chunk(P, j, g.xy, si, wi, wt, lane, S, false);
-        } else {
+            const int lab = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
+            bool direct = false;
+            if (nraw >= 3) {
+                const double4 box = make_double4(g.pd[0] - si.x, g.pd[1] - si.x, g.pd[2] - si.y, g.pd[3] - si.y);
+                const RegPoly Q = ring_from_cache(lab, ncache, g.xy, box, si, wi, wt, lane, S);
+                if (Q.nv != -2) {
+                    P = Q;
+                    direct = true;
+                }
+            }
+            PSTAT_ADD(12, direct ? 1 : 0);
+            if (!direct) {
+                const int j = (lane < ncache && lab >= 0) ? lab : -1;
+                P = apply_chunk(P, j, g.xy, si, wi, wt, lane, S, false);
+            }
+            // a hidden cell that reappears gets the window as well, so that
+            // the certificate starts from a tight ring
+            if (hidden && P.nv > 0) cached = false;
+        }
+        if (!cached && P.nv > 0) {
             int bcnt = 0, bst = 0;
             if (lane < 9) {
                 const int du = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
@@ -1309,12 +1425,27 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
             if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(S, nv, si, a.solid_z, a.solid_light) : 0.0;
         }
         if (a.nbn != nullptr) {
-            // neighbours of this evaluation seed the next one
-            const bool isn = lane < nv && P.l >= 0;
-            const unsigned m = __ballot_sync(FULLMASK, isn);
-            const int pos = __popc(m & ((1u << lane) - 1u));
-            if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = P.l;
-            if (lane == 0) a.nbn[i] = min(__popc(m), COT_NBC);
+            // this evaluation seeds the next: a ring of up to COT_NBC edges
+            // in order (domain sides included); else its sites, or for a
+            // hidden cell the site that emptied its ring and that ring's sites
+            if (nv >= 3 && nv <= COT_NBC) {
+                if (lane < nv) a.nbc[(size_t)i * COT_NBC + lane] = P.l;
+                if (lane == 0) a.nbn[i] = nv;
+            } else {
+                int lab = lane < nv ? P.l : -1;
+                if (nv == 0) {
+                    __syncwarp();
+                    const int kn = S.kn;
+                    lab = -1;
+                    if (kn >= 0) lab = lane == 0 ? S.kill : (lane - 1 < kn ? S.KL[lane - 1] : -1);
+                }
+                const bool isn = lab >= 0;
+                const unsigned m = __ballot_sync(FULLMASK, isn);
+                const int pos = __popc(m & ((1u << lane) - 1u));
+                if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = lab;
+                const int cnt = min(__popc(m), COT_NBC);
+                if (lane == 0) a.nbn[i] = cnt == 0 ? 0 : (nv == 0 ? -(COT_NB_HIDDEN + cnt) : -cnt);
+            }
         }
         if (lane == 0) {
             a.mu[i] = acc.mu;
@@ -1385,10 +1516,14 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
         const int bu = bi % g.bx, bv = bi / g.bx;
         // ---- 1. first candidates: the cell's neighbours at the previous
         //         evaluation, or the 3x3 buckets around the site ---------------
-        const int ncache = (a.nbn != nullptr) ? a.nbn[i] : 0;
+        // cache entries: +m ordered ring (domain sides -1..-4 skipped here),
+        // -m unordered sites, -(COT_NB_HIDDEN + m) the sites that hid the cell
+        const int nraw = (a.nbn != nullptr) ? a.nbn[i] : 0;
+        const int ncache = min(nraw >= 0 ? nraw : (nraw < -COT_NB_HIDDEN ? -nraw - COT_NB_HIDDEN : -nraw), COT_NBC);
         const bool cached = ncache > 0;
         if (cached) {
             int j = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
+            if (j < 0) j = -1;
             nv = clip_chunk<MAXV>(P, nv, j, g, si, wi, wt, lane, status, false);
         } else {
             int bcnt = 0, bst = 0;
@@ -1565,7 +1700,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
             unsigned m = __ballot_sync(FULLMASK, isn);
             int pos = __popc(m & ((1u << lane) - 1u));
             if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = lab;
-            if (lane == 0) a.nbn[i] = min(__popc(m), COT_NBC);
+            if (lane == 0) a.nbn[i] = -min(__popc(m), COT_NBC);
         }
         if (lane == 0) {
             a.mu[i] = acc.mu;
