@@ -208,8 +208,11 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     p, cfg = workload(args.config)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
-    solver = capi.Solver(device=local, profile=True)
+    # a stream of our own: the legacy default stream cannot be captured, and
+    # the solve runs its trial loop as one CUDA graph
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    solver = capi.Solver(device=local)
     solver.set_stream(stream.cuda_stream)
     xy_d = torch.from_numpy(p.xy.reshape(-1)).to(dev)
     nu_d = torch.from_numpy(p.nu).to(dev)
@@ -256,17 +259,28 @@ def run_ours(args):
         cell_evals = float(c.item())
     value = cell_evals / (tot_ms * 1e-3)
 
-    # roofline of the fused cell kernel
+    # roofline of the fused cell kernel: CUDA events around every launch need
+    # the host-driven trial loop (graph-captured launches carry no per-launch
+    # events), so one more solve of the same workload runs that way, on the
+    # same stream, right after the timed region
+    prof = capi.Solver(device=local, profile=True)
+    prof.set_stream(stream.cuda_stream)
+    prof.set_problem(xy_d, nu_d, pic_d, p.size, p.proj_domain)
+    flush.fill_(7)
+    prof.solve(w0, mode=capi.SOLVE_WOLFE, history=args.history, max_iter=100000, tol=args.tol, use_graph=-1)
+    kp = prof.kernel_stats(reset=True)
+    prof.close()
     hbm, peak_kind = peaks()
     H, W = p.size[1], p.size[0]
     alg_bytes = 8.0 * H * W + 48.0 * p.n
-    avg_ms = ks["cell_ms"] / max(ks["cell_launches"], 1)
+    avg_ms = kp["cell_ms"] / max(kp["cell_launches"], 1)
     achieved = alg_bytes / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else None
     traffic = committed_traffic()
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
             "kernel": "k_cells_fast (fused power cell + pixel integration)",
-            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms, "launches": ks["cell_launches"],
+            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms, "launches": kp["cell_launches"],
+            "timing": "CUDA events around each launch, one host-driven solve of the same workload",
             "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"}
 
     # end to end through the public API with host buffers

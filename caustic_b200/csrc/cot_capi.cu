@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstddef>
 #include <cstring>
+#include <climits>
 #include <string>
 #include <vector>
 
@@ -831,6 +832,73 @@ static int report_progress(cot_handle *h, int phase, int iteration, int status, 
     return COT_OK;
 }
 
+// Counters that one body of the trial graph adds per execution.
+struct BodyCounts {
+    long long launches = 0, cell_launches = 0, evaluations = 0;
+};
+
+// The trial loop as one CUDA graph: a WHILE node whose body is one line-search
+// trial -- begin + direction (no-ops inside a line search), the evaluation,
+// the reduction with its line-search decision, accept / reject (no-ops unless
+// the line search just ended) and the loop condition.  The whole solve then
+// runs on the device without a host round trip per trial; the host looks
+// again only when the loop stops (done, or a progress report is due).
+// Returns COT_OK with *exec set, or an error (the caller then runs the
+// host-driven loop).
+static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec, BodyCounts *bc)
+{
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    *exec = nullptr;
+    if (s == nullptr || s == cudaStreamLegacy) return COT_EINVAL;  // the legacy stream cannot be captured
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) return COT_ECUDA;
+    cudaGraphConditionalHandle hc;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hc;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                            cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        return COT_ECUDA;
+    }
+    // counters and per-launch event timing stay out of the captured body
+    CotCtx &c = h->c();
+    const CotCtx saved = c;
+    c.profile = false;
+    launch_begin_iteration(P.S, c);
+    launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, c);
+    CellsArgs a = cells_args(P, P.w, P.d, tptr);
+    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, c);
+    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, c);
+    launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, c);
+    launch_reject(P.S, c);
+    launch_loop_cond(hc, P.S, c);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(s, &captured);
+    bc->launches = c.launches - saved.launches;
+    bc->cell_launches = c.cell_launches - saved.cell_launches;
+    bc->evaluations = c.evaluations - saved.evaluations;
+    c = saved;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *exec = nullptr;
+        cudaGetLastError();
+        return COT_ECUDA;
+    }
+    return COT_OK;
+}
+
 static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms, int phase,
                         bool report_start)
 {
@@ -863,6 +931,8 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
     hs.tol = o.tol;
     hs.H0 = 1.0;
     hs.f = INFINITY;
+    hs.need_begin = 1;
+    hs.pause_iter = INT_MAX;
     if (o.max_iter == 0) hs.done = 1;
     COT_CUDA_TRY(cudaMemcpyAsync(P.S, &hs, sizeof(CotSolver), cudaMemcpyHostToDevice, s));
     cudaEvent_t e0, e1;
@@ -895,43 +965,87 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
     const size_t ctl = 16 * sizeof(int);
     int reported = 0;
     double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
-    while (true) {
-        launch_begin_iteration(P.S, h->c());
-        launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, h->c());
+    // progress report at an iteration boundary (hs holds the control block)
+    auto boundary_report = [&]() -> int {
+        if (!(h->prog_fn && hs.iter > 0 && hs.iter != reported && ((hs.iter - 1) % h->prog_every == 0 || hs.done)))
+            return COT_OK;
+        // iteration hs.iter - 1 is complete; the whole control block carries
+        // its |g| and max-rel figures
+        reported = hs.iter;
+        COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
+        COT_CUDA_TRY(cudaStreamSynchronize(s));
+        const CotSolver snap = hs;
+        const int status = !snap.done ? 0 : (snap.converged ? 1 : 2);
+        int r = report_progress(h, phase, snap.iter - 1, status, std::sqrt(snap.gnorm2), snap.maxrel);
+        hs = snap;
+        return r;
+    };
+    auto stop = [&](int r) -> int {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        out = hs;
+        if (ms) *ms = 0.0f;
+        return r;
+    };
+    cudaGraphExec_t exec = nullptr;
+    BodyCounts bc;
+    if (o.use_graph >= 0 && build_trial_graph(h, tptr, &exec, &bc) == COT_OK) {
+        // device-driven loop: one graph launch runs trials until the solve is
+        // done or the next progress report is due
         COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
         COT_CUDA_TRY(cudaStreamSynchronize(s));
-        if (h->prog_fn && hs.iter > 0 && hs.iter != reported && ((hs.iter - 1) % h->prog_every == 0 || hs.done)) {
-            // iteration hs.iter - 1 is complete; the whole control block
-            // carries its |g| and max-rel figures
-            reported = hs.iter;
-            COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
-            COT_CUDA_TRY(cudaStreamSynchronize(s));
-            const CotSolver snap = hs;
-            const int status = !snap.done ? 0 : (snap.converged ? 1 : 2);
-            int r = report_progress(h, phase, snap.iter - 1, status, std::sqrt(snap.gnorm2), snap.maxrel);
-            hs = snap;
-            if (r != COT_OK) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                out = hs;
-                if (ms) *ms = 0.0f;
-                return r;
+        const int evals0 = hs.evals;
+        int r = COT_OK;
+        while (!hs.done && r == COT_OK) {
+            int pause = INT_MAX;
+            if (h->prog_fn) {
+                // iteration k (k a multiple of every) completes at iter k+1
+                const int every = h->prog_every;
+                pause = ((hs.iter + every - 1) / every) * every + 1;
             }
+            hs.pause_iter = pause;
+            cudaError_t e = cudaMemcpyAsync(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, pause_iter),
+                                            &hs.pause_iter, sizeof(int), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) {
+                r = fail(h, COT_ECUDA, "solve: trial graph", cudaGetErrorString(e));
+                break;
+            }
+            r = boundary_report();
         }
-        if (hs.done) break;
+        const long long bodies = hs.evals - evals0;
+        h->ctx.launches += bodies * bc.launches;
+        h->ctx.cell_launches += bodies * bc.cell_launches;
+        h->ctx.evaluations += bodies * bc.evaluations;
+        cudaGraphExecDestroy(exec);
+        if (r != COT_OK) return stop(r);
+    } else {
+        // host-driven loop: one control-block read per trial
         while (true) {
-            CellsArgs a = cells_args(P, P.w, P.d, tptr);
-            launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
-            launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, h->c());
+            launch_begin_iteration(P.S, h->c());
+            launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, h->c());
             COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
             COT_CUDA_TRY(cudaStreamSynchronize(s));
-            if (!hs.ls_active) break;
+            int r = boundary_report();
+            if (r != COT_OK) return stop(r);
+            if (hs.done) break;
+            while (true) {
+                CellsArgs a = cells_args(P, P.w, P.d, tptr);
+                launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+                launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S,
+                              h->c());
+                COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
+                COT_CUDA_TRY(cudaStreamSynchronize(s));
+                if (!hs.ls_active) break;
+            }
+            if (hs.accepted)
+                launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, h->c());
+            else
+                launch_reject(P.S, h->c());
+            COT_CUDA_TRY(cudaGetLastError());
         }
-        if (hs.accepted)
-            launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, h->c());
-        else
-            launch_reject(P.S, h->c());
-        COT_CUDA_TRY(cudaGetLastError());
     }
     COT_CUDA_TRY(cudaEventRecord(e1, s));
     COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));

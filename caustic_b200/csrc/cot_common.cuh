@@ -71,7 +71,9 @@ struct CotSolver {
     int restart;         // reference's restart flag
     int trials;
     int final_eval;      // Wolfe: the pending trial re-evaluates lo
-    int ctl_pad[3];
+    int need_begin;      // 1 at an iteration boundary (set by accept / reject)
+    int eval_mark;       // evals when the iteration began (direction pending while equal)
+    int pause_iter;      // graph solve: the device loop stops when iter reaches this
     // options
     int mode;            // COT_SOLVE_*
     int m;               // history
@@ -160,6 +162,7 @@ void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double
                    const double *wt, double *mu, const double *mut, const double *d,
                    double *partials, unsigned int *ticket, int initial, CotCtx &c);
 void launch_reject(CotSolver *S, CotCtx &c);
+void launch_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S, CotCtx &c);
 void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c);
 void configure_cells_kernels();
 void launch_fcell_full(int n, const double *fc, const double *wt, const double *nu, double *out, CotCtx &c);

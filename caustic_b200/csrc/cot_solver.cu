@@ -214,7 +214,11 @@ __device__ __forceinline__ double gram_dot(const CotSolver *S, int row, const do
 __global__ void k_begin_iteration(CotSolver *S)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (S->done) return;
+    // only at an iteration boundary: inside a device-driven loop this kernel
+    // also runs before every further trial of a line search
+    if (S->done || !S->need_begin) return;
+    S->need_begin = 0;
+    S->eval_mark = S->evals;
     const int m = S->m, gi = 2 * m;
     S->gnorm_stale = sqrt(S->gnorm2);
     S->empty_stale = S->empty;
@@ -266,7 +270,8 @@ __global__ void k_direction(int n, const CotSolver *__restrict__ S, const double
                             const double *__restrict__ Yv, const double *__restrict__ mu,
                             const double *__restrict__ nu, double *__restrict__ d)
 {
-    if (S->done) return;
+    // only right after k_begin_iteration (no trial evaluated since)
+    if (S->done || S->evals != S->eval_mark || !S->ls_active) return;
     __shared__ double dl[COT_BASIS];
     const int m = S->m;
     for (int c = threadIdx.x; c < 2 * m + 1; c += blockDim.x) dl[c] = S->delta[c];
@@ -302,7 +307,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
                                                        const double *__restrict__ d, double *partials,
                                                        unsigned int *ticket, int initial)
 {
-    __shared__ double sh[33];
+    constexpr int NW = RED_THREADS / 32;
+    __shared__ double red[(5 * COT_MAX_HIST + 1) * NW];
+    __shared__ double tot[5 * COT_MAX_HIST + 1];
     __shared__ bool last;
     if (S->done) return;
     if (!initial && !S->accepted) return;
@@ -310,9 +317,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
     const int h = S->k % m;
     const double t = S->t;
     const int nvals = 5 * m + 1;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int per = (n + gridDim.x - 1) / gridDim.x;
     int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
-    // new vectors
+    // new vectors (each thread later reads back only what it wrote)
     for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
         double mt = mut[i];
         if (!initial) {
@@ -322,17 +330,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
         }
         mu[i] = mt;
     }
-    __syncthreads();
     int cnt = initial ? 0 : (S->k + 1 < m ? S->k + 1 : m);  // slots that hold pairs after this update
+    // all 5m+1 sums in one sweep: per-warp partials in shared memory, summed
+    // in warp order, then block partials summed in block order by the last
+    // block (the order of a per-value block reduction, in one barrier)
     for (int j = 0; j < m; j++) {
         double sy = 0.0, ys = 0.0, yy = 0.0, gs = 0.0, gy = 0.0;
-        bool valid = false;
-        if (cnt > 0) {
-            // slot j is valid if it is among the last cnt slots ending at h
-            int age = ((h - j) % m + m) % m;
-            valid = age < cnt;
-        }
-        if (valid) {
+        const int age = ((h - j) % m + m) % m;
+        if (cnt > 0 && age < cnt) {
             for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
                 double sj = Sv[(size_t)j * n + i], yj = Yv[(size_t)j * n + i];
                 double sn = Sv[(size_t)h * n + i], yn = Yv[(size_t)h * n + i];
@@ -343,15 +348,18 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
                 gs += g * sj;
                 gy += g * yj;
             }
+            sy = wsum(sy);
+            ys = wsum(ys);
+            yy = wsum(yy);
+            gs = wsum(gs);
+            gy = wsum(gy);
         }
-        double r0 = block_reduce<false>(sy, sh);
-        double r1 = block_reduce<false>(ys, sh);
-        double r2 = block_reduce<false>(yy, sh);
-        double r3 = block_reduce<false>(gs, sh);
-        double r4 = block_reduce<false>(gy, sh);
-        if (threadIdx.x == 0) {
-            double *pp = partials + (size_t)blockIdx.x * nvals + 5 * j;
-            pp[0] = r0; pp[1] = r1; pp[2] = r2; pp[3] = r3; pp[4] = r4;
+        if (lane == 0) {
+            red[(5 * j + 0) * NW + wid] = sy;
+            red[(5 * j + 1) * NW + wid] = ys;
+            red[(5 * j + 2) * NW + wid] = yy;
+            red[(5 * j + 3) * NW + wid] = gs;
+            red[(5 * j + 4) * NW + wid] = gy;
         }
     }
     double gg = 0.0;
@@ -359,10 +367,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
         double g = mu[i] - nu[i];
         gg += g * g;
     }
-    double rg = block_reduce<false>(gg, sh);
+    gg = wsum(gg);
+    if (lane == 0) red[5 * m * NW + wid] = gg;
+    __syncthreads();
+    for (int v = threadIdx.x; v < nvals; v += blockDim.x) {
+        double r = 0.0;
+        for (int k = 0; k < NW; k++) r += red[v * NW + k];
+        partials[(size_t)blockIdx.x * nvals + v] = r;
+    }
+    __threadfence();
+    __syncthreads();
     if (threadIdx.x == 0) {
-        partials[(size_t)blockIdx.x * nvals + 5 * m] = rg;
-        __threadfence();
         unsigned int tk = atomicAdd(ticket, 1u);
         last = (tk == gridDim.x - 1);
     }
@@ -370,7 +385,6 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
     if (!last) return;
     __threadfence();
     volatile double *p = partials;
-    __shared__ double tot[5 * COT_MAX_HIST + 1];
     for (int v = threadIdx.x; v < nvals; v += blockDim.x) {
         double r = 0.0;
         for (unsigned b = 0; b < gridDim.x; b++) r += p[(size_t)b * nvals + v];
@@ -413,6 +427,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
         S->k++;
     }
     S->iter++;
+    S->need_begin = 1;
     if (S->mode == COT_SOLVE_REFERENCE) {
         if (S->gnorm_stale < S->tol && S->empty_stale == 0) { S->converged = 1; S->done = 1; }
     } else {
@@ -433,7 +448,8 @@ void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double
 // Line search gave up (ot_op.cuh:413-425): keep the point, drop the history.
 __global__ void k_reject(CotSolver *S)
 {
-    if (S->done || S->accepted) return;
+    if (S->done || S->accepted || S->ls_active) return;
+    S->need_begin = 1;
     if (S->mode == COT_SOLVE_REFERENCE) {
         S->restart = 1;
     } else if (S->k == 0) {
@@ -451,6 +467,20 @@ __global__ void k_reject(CotSolver *S)
 void launch_reject(CotSolver *S, CotCtx &c)
 {
     k_reject<<<1, 1, 0, c.s>>>(S);
+    c.launches++;
+}
+
+// Condition of the device-driven trial loop (a WHILE node of a CUDA graph):
+// go on until the solve is done or reaches the iteration where the host
+// wants to look (a progress report).
+__global__ void k_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S)
+{
+    cudaGraphSetConditional(hc, (!S->done && S->iter < S->pause_iter) ? 1u : 0u);
+}
+
+void launch_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S, CotCtx &c)
+{
+    k_loop_cond<<<1, 1, 0, c.s>>>(hc, S);
     c.launches++;
 }
 

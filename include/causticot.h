@@ -97,7 +97,13 @@ typedef struct {
     double initial_step; /* reference: initial_step */
     double c1, c2;       /* Wolfe constants (0: 1e-4, 0.9) */
     int max_ls;          /* line-search trials per iteration (0: 30) */
-    int use_graph;       /* 1: run the iteration loop as a CUDA graph */
+    int use_graph;       /* >= 0 (default): the trial loop runs on the device
+                            as one CUDA graph (a WHILE node, one line-search
+                            trial per pass; the host looks only when it stops),
+                            or the host-driven loop if the handle's stream
+                            cannot be captured (the legacy default stream);
+                            -1: the host-driven loop, one 64-byte control-block
+                            read per trial */
 } cot_solve_opts;
 
 typedef struct {

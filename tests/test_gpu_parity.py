@@ -337,3 +337,26 @@ def test_reference_run_on_gpu(gpu):
     ov = np.array([[float(a[1]), float(a[2])] for a in sub])
     d = np.abs(c[oi] - ov)
     assert np.median(d) < 5e-4 and np.percentile(d, 99) < 1e-2 and d.max() < 3e-2
+
+
+@pytest.mark.parametrize("mode", [capi.SOLVE_WOLFE, capi.SOLVE_REFERENCE])
+def test_graph_loop_matches_host_loop(gpu, mode):
+    """The device-driven trial loop (one CUDA graph, a WHILE node per trial)
+    takes the same decisions as the host-driven one: same counts, same bits."""
+    p = problems.make(1, g=24, res=96, beam=True)
+    a = solver_for(p)
+    wg, sg = a.solve(np.zeros(p.n), mode=mode, tol=1e-5 if mode == capi.SOLVE_REFERENCE else 1e-4, history=7,
+                     max_iter=3000, use_graph=0)
+    b = solver_for(p)
+    wh, sh = b.solve(np.zeros(p.n), mode=mode, tol=1e-5 if mode == capi.SOLVE_REFERENCE else 1e-4, history=7,
+                     max_iter=3000, use_graph=-1)
+    assert sg.converged and sh.converged
+    assert (sg.iterations, sg.evaluations, sg.restarts) == (sh.iterations, sh.evaluations, sh.restarts)
+    assert np.array_equal(wg, wh)
+    # the launch accounting of the graph counts every kernel of every pass
+    ka, kb = a.kernel_stats(), b.kernel_stats()
+    assert ka["evaluations"] == kb["evaluations"] and ka["cell_launches"] == kb["cell_launches"]
+    # a solve cut short by max_iter stops at the same point
+    wg2, sg2 = solver_for(p).solve(np.zeros(p.n), mode=mode, tol=1e-12, history=7, max_iter=37, use_graph=0)
+    wh2, sh2 = solver_for(p).solve(np.zeros(p.n), mode=mode, tol=1e-12, history=7, max_iter=37, use_graph=-1)
+    assert sg2.iterations == sh2.iterations == 37 and np.array_equal(wg2, wh2)
