@@ -53,6 +53,8 @@ def parse():
                     help="oracle evaluations per CPU sample (about 1 s each at the default size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cells-per-warp", type=int, default=0, help="1 or 2 (0: the library default)")
+    ap.add_argument("--bucket-size", type=int, default=0, help="sites per neighbour bucket (0: the library default)")
     return ap.parse_args()
 
 
@@ -212,7 +214,8 @@ def run_ours(args):
     # the solve runs its trial loop as one CUDA graph
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
-    solver = capi.Solver(device=local)
+    kw = dict(cells_per_warp=args.cells_per_warp, bucket_size=args.bucket_size)
+    solver = capi.Solver(device=local, **kw)
     solver.set_stream(stream.cuda_stream)
     xy_d = torch.from_numpy(p.xy.reshape(-1)).to(dev)
     nu_d = torch.from_numpy(p.nu).to(dev)
@@ -263,7 +266,7 @@ def run_ours(args):
     # the host-driven trial loop (graph-captured launches carry no per-launch
     # events), so one more solve of the same workload runs that way, on the
     # same stream, right after the timed region
-    prof = capi.Solver(device=local, profile=True)
+    prof = capi.Solver(device=local, profile=True, **kw)
     prof.set_stream(stream.cuda_stream)
     prof.set_problem(xy_d, nu_d, pic_d, p.size, p.proj_domain)
     flush.fill_(7)
@@ -290,7 +293,7 @@ def run_ours(args):
         nu_h = torch.from_numpy(p.nu).pin_memory()
         pic_h = torch.from_numpy(p.picture).pin_memory()
         w_h = torch.zeros(p.n, dtype=torch.float64).pin_memory()
-        s2 = capi.Solver(device=local)
+        s2 = capi.Solver(device=local, **kw)
         s2.set_stream(stream.cuda_stream)
         # warm the handle once
         s2.set_problem(xy_h.numpy(), nu_h.numpy(), pic_h.numpy(), p.size, p.proj_domain)

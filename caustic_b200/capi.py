@@ -53,7 +53,7 @@ NOALLOC_MAX_N = 2048 * 1024
 
 class cot_config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("bucket_size", ctypes.c_int),
-                ("warps_per_block", ctypes.c_int), ("max_ring", ctypes.c_int), ("profile", ctypes.c_int)]
+                ("cells_per_warp", ctypes.c_int), ("max_ring", ctypes.c_int), ("profile", ctypes.c_int)]
 
 
 class cot_kernel_stats(ctypes.Structure):
@@ -166,11 +166,11 @@ class Solver:
     contiguous); outputs come back in the same kind as the input weights.
     """
 
-    def __init__(self, device: int = 0, bucket_size: int = 0, warps_per_block: int = 0, max_ring: int = 0,
+    def __init__(self, device: int = 0, bucket_size: int = 0, cells_per_warp: int = 0, max_ring: int = 0,
                  profile: bool = False):
         L = load()
         self._L = L
-        cfg = cot_config(device, bucket_size, warps_per_block, max_ring, int(bool(profile)))
+        cfg = cot_config(device, bucket_size, cells_per_warp, max_ring, int(bool(profile)))
         h = ctypes.c_void_p()
         rc = L.cot_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != COT_OK:

@@ -36,7 +36,7 @@ struct CotProblemDev {
     double *w = nullptr, *wt = nullptr, *d = nullptr, *mu = nullptr, *mut = nullptr, *fc = nullptr;
     double *wq = nullptr;  // weights of the query entry points, apart from a solve's iterate w
     double *phibar = nullptr;
-    int *nv = nullptr, *ovf_list = nullptr, *ovf_count = nullptr;
+    int *nv = nullptr, *ovf_list = nullptr, *ovf_list2 = nullptr, *ovf_count = nullptr;
     int *nbc = nullptr, *nbn = nullptr;        // neighbour cache of the solves
     int *nbc_q = nullptr, *nbn_q = nullptr;    // and of the query entry points
     double *partials = nullptr;
@@ -134,7 +134,7 @@ using namespace cot;
 static void free_problem(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
-                    P.wq, P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
+                    P.wq, P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
                     P.Yv};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -157,8 +157,11 @@ extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
     if (!h) return fail(nullptr, COT_ENOMEM, "cot_create: out of host memory", nullptr);
     if (cfg) h->cfg = *cfg;
     if (h->cfg.bucket_size <= 0) h->cfg.bucket_size = 16;
-    if (h->cfg.warps_per_block <= 0) h->cfg.warps_per_block = 4;
-    if (h->cfg.warps_per_block > 8) h->cfg.warps_per_block = 8;
+    if (h->cfg.cells_per_warp <= 0) h->cfg.cells_per_warp = 1;
+    if (h->cfg.cells_per_warp != 1 && h->cfg.cells_per_warp != 2) {
+        delete h;
+        return failf(nullptr, COT_EINVAL, "cot_create: cells_per_warp must be 1 or 2");
+    }
     if (h->cfg.max_ring <= 0) h->cfg.max_ring = 200;
     h->device = h->cfg.device;
     int ndev = 0;
@@ -419,7 +422,8 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
     if (e == cudaSuccess) e = A((void **)&P.nv, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.ovf_list, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.ovf_count, 4 * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.ovf_list2, N * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.ovf_count, 8 * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbc, N * COT_NBC * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbn, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
@@ -441,7 +445,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
-    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 4 * sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 8 * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
@@ -551,8 +555,8 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.fc = P.fc;
     a.nv = P.nv;
     a.ovf_list = P.ovf_list;
+    a.ovf_list2 = P.ovf_list2;
     a.ovf_count = P.ovf_count;
-    a.work = P.ovf_count + 1;
     // the query entry points (weights in P.wq) keep their own neighbour cache
     // so that a query made during a solve does not change the solve's clip
     // order
@@ -574,7 +578,7 @@ extern "C" int cot_eval(cot_handle *h, const double *w, double *f_total, double 
     int r;
     if ((r = upload_sorted(h, w, mem, P.wq)) != COT_OK) return r;
     CellsArgs a = cells_args(P, P.wq, nullptr, nullptr);
-    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+    launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
     launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
     COT_CUDA_TRY(cudaGetLastError());
     CotEvalOut o;
@@ -624,7 +628,7 @@ extern "C" int cot_cells(cot_handle *h, const double *w, int *ring_offsets, doub
         a.ring_xy = rxy;
         a.ring_lab = rlab;
         a.ring_cap = cap;
-        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
         hxy.resize(N * cap * 2);
         hlab.resize(N * cap);
         e = cudaMemcpyAsync(hxy.data(), rxy, N * cap * 2 * 8, cudaMemcpyDeviceToHost, s);
@@ -686,7 +690,7 @@ extern "C" int cot_centroids(cot_handle *h, const double *w, double *xy, unsigne
     a.cen = cen;
     a.exist = ex;
     a.weighted = weighted ? 1 : 0;
-    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+    launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
     double *cen2 = cen + 2 * N;
     k_scatter2<<<nblk(P.n), 256, 0, s>>>(P.n, P.perm, cen, cen2);
     k_scatter_u8<<<nblk(P.n), 256, 0, s>>>(P.n, P.perm, ex, ex2);
@@ -726,7 +730,7 @@ static int source_masses_impl(cot_handle *h, const double *points_xy, int n, con
             a.solid_z = z;
             for (int c = 0; c < 3; c++) a.solid_light[c] = light[c];
         }
-        launch_eval(Q.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        launch_eval(Q.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
         e = cudaMemcpyAsync(sorted.data(), light ? solid : Q.mut, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -784,7 +788,7 @@ extern "C" int cot_render(cot_handle *h, const double *w, double gray_multiple, 
         CellsArgs a = cells_args(P, P.wq, nullptr, nullptr);
         a.splat = img;
         a.splat_scale = gray_multiple;
-        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
         e = cudaMemcpyAsync(out, img, npx * 8, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     }
@@ -878,7 +882,7 @@ static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec,
     launch_begin_iteration(P.S, c);
     launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, c);
     CellsArgs a = cells_args(P, P.w, P.d, tptr);
-    launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, c);
+    launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, c);
     launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, c);
     launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, c);
     launch_reject(P.S, c);
@@ -942,7 +946,7 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
     // first point
     {
         CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
-        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
         launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
         launch_init_from_eval(P.S, P.out, h->c());
         launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, h->c());
@@ -1033,7 +1037,7 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
             if (hs.done) break;
             while (true) {
                 CellsArgs a = cells_args(P, P.w, P.d, tptr);
-                launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+                launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
                 launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S,
                               h->c());
                 COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
@@ -1224,7 +1228,7 @@ extern "C" int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inp
         a.cen = cen;
         a.exist = ex;
         a.weighted = 0;
-        launch_eval(P.geo, a, h->cfg.warps_per_block, h->num_sms, h->c());
+        launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
         evals++;
         // ring check first (polygons_in_VD + the max_edge_num/2 test)
         launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());

@@ -34,16 +34,19 @@ namespace cot {
 // Measurement build only: per-phase cycle and event counters, kept per warp
 // in shared memory and added to the global totals once when the warp exits.
 __device__ unsigned long long cot_phase_stats[16];
-__shared__ unsigned long long cot_pst[8][16];
-#define PSTAT_ADD(k, v) do { if ((threadIdx.x & 31) == 0) cot_pst[threadIdx.x >> 5][k] += (unsigned long long)(v); } while (0)
+// (per segment of LPC lanes: LPC must be a constant in scope where they are used)
+__shared__ unsigned long long cot_pst[16][16];
+#define PSTAT_ADD(k, v) do { if ((threadIdx.x & (LPC - 1)) == 0) cot_pst[threadIdx.x / LPC][k] += (unsigned long long)(v); } while (0)
 #define PSTAT_CLOCK(var) long long var = clock64()
-#define PSTAT_INIT() do { if ((threadIdx.x & 31) == 0) for (int q_ = 0; q_ < 16; q_++) cot_pst[threadIdx.x >> 5][q_] = 0; } while (0)
-#define PSTAT_FLUSH() do { if ((threadIdx.x & 31) == 0) for (int q_ = 0; q_ < 16; q_++) atomicAdd(&cot_phase_stats[q_], cot_pst[threadIdx.x >> 5][q_]); } while (0)
+#define PSTAT_INIT() do { if ((threadIdx.x & (LPC - 1)) == 0) for (int q_ = 0; q_ < 16; q_++) cot_pst[threadIdx.x / LPC][q_] = 0; } while (0)
+#define PSTAT_FLUSH() do { if ((threadIdx.x & (LPC - 1)) == 0) for (int q_ = 0; q_ < 16; q_++) atomicAdd(&cot_phase_stats[q_], cot_pst[threadIdx.x / LPC][q_]); } while (0)
+#define PSTAT_LPC32 constexpr int LPC = 32
 #else
 #define PSTAT_INIT() do { } while (0)
 #define PSTAT_FLUSH() do { } while (0)
 #define PSTAT_ADD(k, v) do { } while (0)
 #define PSTAT_CLOCK(var) do { } while (0)
+#define PSTAT_LPC32 do { } while (0)
 #endif
 #define COT_WIN 1  // window radius in buckets
 // neighbour cache count nbn[i]: +m an ordered ring of m generators, -m an
@@ -214,6 +217,69 @@ __device__ __forceinline__ double warp_max(double v)
     return v;
 }
 
+// A segment of LPC lanes working on one cell (LPC = 32: the whole warp).  A
+// warp holds 32 / LPC cells; each segment synchronises, shuffles and votes
+// within its own lanes only.
+template <int LPC>
+struct Seg {
+    static_assert(LPC == 32 || LPC == 16, "lanes per cell: 32 or 16");
+    static constexpr unsigned low = LPC == 32 ? FULLMASK : ((1u << (LPC & 31)) - 1u);
+    unsigned mask;  // the segment's lanes in the warp
+    int base;       // its first lane
+    int sl;         // this lane's index in the segment
+    __device__ __forceinline__ Seg()
+    {
+        const int lane = threadIdx.x & 31;
+        base = lane & ~(LPC - 1);
+        sl = lane & (LPC - 1);
+        mask = low << base;
+    }
+    __device__ __forceinline__ unsigned ballot(bool p) const { return (__ballot_sync(mask, p) >> base) & low; }
+    __device__ __forceinline__ bool any(bool p) const { return ballot(p) != 0u; }
+    __device__ __forceinline__ bool all(bool p) const { return ballot(p) == low; }
+    template <class T>
+    __device__ __forceinline__ T shfl(T v, int src) const { return __shfl_sync(mask, v, src, LPC); }
+    template <class T>
+    __device__ __forceinline__ T shfl_xor(T v, int o) const { return __shfl_xor_sync(mask, v, o, LPC); }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+    __device__ __forceinline__ unsigned below(int n) const { return n >= LPC ? low : ((1u << n) - 1u); }
+    __device__ __forceinline__ int incl_scan(int v) const
+    {
+#pragma unroll
+        for (int o = 1; o < LPC; o <<= 1) {
+            int t = __shfl_up_sync(mask, v, o, LPC);
+            if (sl >= o) v += t;
+        }
+        return v;
+    }
+    // butterfly reductions: for LPC = 32 the same order as the warp versions
+    __device__ __forceinline__ double sum(double v) const
+    {
+#pragma unroll
+        for (int o = LPC / 2; o > 0; o >>= 1) v += shfl_xor(v, o);
+        return v;
+    }
+    __device__ __forceinline__ double min(double v) const
+    {
+#pragma unroll
+        for (int o = LPC / 2; o > 0; o >>= 1) v = fmin(v, shfl_xor(v, o));
+        return v;
+    }
+    __device__ __forceinline__ double max(double v) const
+    {
+#pragma unroll
+        for (int o = LPC / 2; o > 0; o >>= 1) v = fmax(v, shfl_xor(v, o));
+        return v;
+    }
+    __device__ __forceinline__ int imin(int v) const
+    {
+#pragma unroll
+        for (int o = LPC / 2; o > 0; o >>= 1) v = ::min(v, shfl_xor(v, o));
+        return v;
+    }
+};
+
+
 // Intersection of lines a1 x + b1 y = c1 and a2 x + b2 y = c2.  Axis-aligned
 // lines are solved directly so that vertices on the domain sides sit exactly on
 // them.  Returns false for (near) parallel lines.
@@ -365,6 +431,7 @@ template <int MAXV>
 __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, double2 si, double wi,
                           const double *__restrict__ wt, int lane, int &status, bool check_dup)
 {
+    PSTAT_LPC32;
     bool act = j >= 0;
     if (act && check_dup) {
         // a site whose line already bounds the polygon must not clip again
@@ -531,6 +598,7 @@ __device__ PixGeo splat_geo(const CotGeo &g, const CellsArgs &a, const SP &P, in
 template <class SP>
 __device__ __noinline__ CellAcc integrate_cell(SP &P, int nv, const PixGeo g, double2 si, int lane)
 {
+    PSTAT_LPC32;
     CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
     // per-edge reciprocals and slopes: no divisions in the pixel loop
     for (int k = lane; k < nv; k += 32) {
@@ -715,12 +783,13 @@ __device__ double solid_angle_of(const SP &P, int nv, double2 si, double z, cons
 // edges.  Coordinates are taken relative to the centre of the cell's box for
 // accuracy and shifted to the site at the end.  Used when neither centroids
 // (whose reference rule needs per-pixel areas) nor the render are wanted.
-template <class SP>
-__device__ __noinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, double2 si, int lane)
+template <int LPC, class SP>
+__device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, double2 si, int lane)
 {
+    const Seg<LPC> W;
     CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
     double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
-    for (int k = lane; k < nv; k += 32) {
+    for (int k = lane; k < nv; k += LPC) {
         int kn = (k + 1 == nv) ? 0 : k + 1;
         double dx = P.X[kn] - P.X[k], dy = P.Y[kn] - P.Y[k];
         P.EIX[k] = dx != 0.0 ? 1.0 / dx : 0.0;
@@ -729,13 +798,13 @@ __device__ __noinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, do
         mnx = fmin(mnx, P.X[k]); mxx = fmax(mxx, P.X[k]);
         mny = fmin(mny, P.Y[k]); mxy = fmax(mxy, P.Y[k]);
     }
-    mnx = warp_min(mnx); mxx = warp_max(mxx); mny = warp_min(mny); mxy = warp_max(mxy);
-    __syncwarp();
+    mnx = W.min(mnx); mxx = W.max(mxx); mny = W.min(mny); mxy = W.max(mxy);
+    W.sync();
     const double ox = 0.5 * (mnx + mxx), oy = 0.5 * (mny + mxy);  // local origin
     const double cx0 = g.pd0 - si.x, cy0 = g.pd2 - si.y;           // pixel line 0, site frame
     double sA = 0.0, sIa = 0.0, sIb = 0.0, sI2 = 0.0;
     // (a) edge pieces, one lane per edge
-    for (int k = lane; k < nv; k += 32) {
+    for (int k = lane; k < nv; k += LPC) {
         int kn = (k + 1 == nv) ? 0 : k + 1;
         const double px = P.X[k], py = P.Y[k], qx = P.X[kn], qy = P.Y[kn];
         const double dx = qx - px, dy = qy - py;
@@ -820,9 +889,9 @@ __device__ __noinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, do
     ly = max(ly, 0);
     hx = min(hx, g.nx);
     hy = min(hy, g.ny);
-    for (int cxs = lx; cxs < hx; cxs += 32) {
-        const int cw = min(32, hx - cxs);
-        for (int c = lane; c <= cw; c += 32) {
+    for (int cxs = lx; cxs < hx; cxs += LPC) {
+        const int cw = min(LPC, hx - cxs);
+        for (int c = lane; c <= cw; c += LPC) {
             double xl = (double)(cxs + c) * g.xs + cx0;
             double lo, hi;
             section_at(P, nv, xl, lo, hi);
@@ -831,9 +900,9 @@ __device__ __noinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, do
             P.rv[c] = (mnx <= xl && xl < mxx) ? 1 : 0;  // right limit: left side of a pixel
             P.lv[c] = (mnx < xl && xl <= mxx) ? 1 : 0;  // left limit: right side of a pixel
         }
-        __syncwarp();
+        W.sync();
         const int rows = hy - ly, npx = cw * rows;
-        for (int q = lane; q < npx; q += 32) {
+        for (int q = lane; q < npx; q += LPC) {
             const int c = q % cw, rr = q / cw;
             const int ix = cxs + c, iy = ly + rr;
             const double y0 = (double)iy * g.ys + cy0, y1 = (double)(iy + 1) * g.ys + cy0;
@@ -860,12 +929,12 @@ __device__ __noinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, do
             sIb += rho * m.Ib;
             sI2 += rho * m.I2;
         }
-        __syncwarp();
+        W.sync();
     }
-    sA = warp_sum(sA);
-    sIa = warp_sum(sIa);
-    sIb = warp_sum(sIb);
-    sI2 = warp_sum(sI2);
+    sA = W.sum(sA);
+    sIa = W.sum(sIa);
+    sIb = W.sum(sIb);
+    sI2 = W.sum(sI2);
     acc.mu = sA;
     // int |x - s_i|^2 = int |(x - o) + o|^2 in the site frame
     acc.S = sI2 + 2.0 * (ox * sIa + oy * sIb) + (ox * ox + oy * oy) * sA;
@@ -918,17 +987,19 @@ struct RegPoly {
 
 __device__ __forceinline__ unsigned lanes_below(int n) { return n >= 32 ? FULLMASK : ((1u << n) - 1u); }
 
-// Clip by a x + b y <= c.  Returns false when the ring would exceed 32
+// Clip by a x + b y <= c.  Returns false when the ring would exceed LPC
 // vertices.  A convex ring crossed twice is a pure register permutation;
 // any other pattern (rounding on nearly collinear vertices) is compacted
 // through shared memory.
+template <int LPC>
 __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, int lab, int lane, FastScratch &S)
 {
+    const Seg<LPC> W;
     const int nv = P.nv;
     const bool valid = lane < nv;
     const double d = side(a, b, c, P.x, P.y);
-    const unsigned vm = lanes_below(nv);
-    const unsigned outm = __ballot_sync(FULLMASK, valid && d > 0.0);
+    const unsigned vm = W.below(nv);
+    const unsigned outm = W.ballot(valid && d > 0.0);
     if (outm == 0u) return true;
     if (outm == vm) {
         // hidden cell: remember what hid it, to seed the next evaluation
@@ -941,9 +1012,9 @@ __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, 
         return true;
     }
     const int nx = (lane + 1 >= nv) ? 0 : lane + 1;
-    const double xn = __shfl_sync(FULLMASK, P.x, nx);
-    const double yn = __shfl_sync(FULLMASK, P.y, nx);
-    const double dn = __shfl_sync(FULLMASK, d, nx);
+    const double xn = W.shfl(P.x, nx);
+    const double yn = W.shfl(P.y, nx);
+    const double dn = W.shfl(d, nx);
     const bool in = !((outm >> lane) & 1u);
     const bool inn = !((outm >> nx) & 1u);
     const bool cross = valid && (in != inn);
@@ -955,14 +1026,14 @@ __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, 
             iy = P.y + t * (yn - P.y);
         }
     }
-    const unsigned cm = __ballot_sync(FULLMASK, cross);
+    const unsigned cm = W.ballot(cross);
     const int K = __popc(vm & ~outm);
     if (__popc(cm) == 2) {
-        const unsigned em = __ballot_sync(FULLMASK, cross && !in);  // edge entering the half-plane
+        const unsigned em = W.ballot(cross && !in);  // edge entering the half-plane
         const int e = __ffs(em) - 1;
         const int l = __ffs(cm & ~em) - 1;                         // edge leaving it
         const int nn = K + 2;
-        if (nn > 32) return false;
+        if (nn > LPC) return false;
         // new ring: I_e, v_{e+1} .. v_{e+K} (= v_l), I_l
         int src = e;
         if (lane >= 1 && lane <= K) {
@@ -971,14 +1042,14 @@ __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, 
         } else if (lane == K + 1) {
             src = l;
         }
-        const double gx = __shfl_sync(FULLMASK, P.x, src);
-        const double gy = __shfl_sync(FULLMASK, P.y, src);
-        const double ga = __shfl_sync(FULLMASK, P.a, src);
-        const double gb = __shfl_sync(FULLMASK, P.b, src);
-        const double gc = __shfl_sync(FULLMASK, P.c, src);
-        const int gl = __shfl_sync(FULLMASK, P.l, src);
-        const double iex = __shfl_sync(FULLMASK, ix, e), iey = __shfl_sync(FULLMASK, iy, e);
-        const double ilx = __shfl_sync(FULLMASK, ix, l), ily = __shfl_sync(FULLMASK, iy, l);
+        const double gx = W.shfl(P.x, src);
+        const double gy = W.shfl(P.y, src);
+        const double ga = W.shfl(P.a, src);
+        const double gb = W.shfl(P.b, src);
+        const double gc = W.shfl(P.c, src);
+        const int gl = W.shfl(P.l, src);
+        const double iex = W.shfl(ix, e), iey = W.shfl(iy, e);
+        const double ilx = W.shfl(ix, l), ily = W.shfl(iy, l);
         if (lane == 0) {
             P.x = iex; P.y = iey; P.a = ga; P.b = gb; P.c = gc; P.l = gl;
         } else if (lane <= K) {
@@ -990,10 +1061,10 @@ __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, 
         return true;
     }
     const int cnt = valid ? ((in ? 1 : 0) + (cross ? 1 : 0)) : 0;
-    const int inc = warp_incl_scan(cnt, lane);
-    const int tot = __shfl_sync(FULLMASK, inc, 31);
-    if (tot > 32) return false;
-    __syncwarp();
+    const int inc = W.incl_scan(cnt);
+    const int tot = W.shfl(inc, LPC - 1);
+    if (tot > LPC) return false;
+    W.sync();
     if (valid) {
         int p = inc - cnt;
         if (in) {
@@ -1006,24 +1077,26 @@ __device__ __forceinline__ bool rclip(RegPoly &P, double a, double b, double c, 
             else { S.A[p] = P.a; S.B[p] = P.b; S.C[p] = P.c; S.L[p] = P.l; }
         }
     }
-    __syncwarp();
+    W.sync();
     if (lane < tot) {
         P.x = S.X[lane]; P.y = S.Y[lane]; P.a = S.A[lane]; P.b = S.B[lane]; P.c = S.C[lane]; P.l = S.L[lane];
     }
-    __syncwarp();
+    W.sync();
     P.nv = tot;
     return true;
 }
 
-// Ascending bitonic sort of (key, idx) across the warp.
+// Ascending bitonic sort of (key, idx) across the segment.
+template <int LPC>
 __device__ __forceinline__ void warp_sort(double &key, int &idx, int lane)
 {
+    const Seg<LPC> W;
 #pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
+    for (int k = 2; k <= LPC; k <<= 1) {
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
-            double ok = __shfl_xor_sync(FULLMASK, key, j);
-            int oi = __shfl_xor_sync(FULLMASK, idx, j);
+            double ok = W.shfl_xor(key, j);
+            int oi = W.shfl_xor(idx, j);
             bool up = (lane & k) == 0;
             bool lower = (lane & j) == 0;
             bool less = ok < key || (ok == key && oi < idx);
@@ -1038,15 +1111,17 @@ __device__ __forceinline__ void warp_sort(double &key, int &idx, int lane)
 // shared memory); only candidates that cut are then applied one by one with a
 // register clip (one that no longer cuts after an earlier clip is a no-op).
 // `nearest` applies the cutting ones in order of distance from the site.
-__device__ __noinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__restrict__ sxy, double2 si, double wi,
+template <int LPC>
+__device__ __forceinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__restrict__ sxy, double2 si, double wi,
                                             const double *__restrict__ wt, int lane, FastScratch &S, bool nearest)
 {
-    if (__ballot_sync(FULLMASK, jl >= 0) == 0u) return P;
+    const Seg<LPC> W;
+    if (W.ballot(jl >= 0) == 0u) return P;
     double al = 0.0, bl = 0.0, cl = 0.0, key = INFINITY;
     if (jl >= 0) site_line(sxy[jl], si, wt[jl], wi, al, bl, cl, key);
     const int nv = P.nv;
     if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; S.L[lane] = P.l; }
-    __syncwarp();
+    W.sync();
     bool cut = false;
     if (jl >= 0) {
         for (int k = 0; k < nv; k++) {
@@ -1054,31 +1129,31 @@ __device__ __noinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__
             if (side(al, bl, cl, S.X[k], S.Y[k]) > 0.0) cut = true;
         }
     }
-    __syncwarp();
-    unsigned have = __ballot_sync(FULLMASK, cut);
+    W.sync();
+    unsigned have = W.ballot(cut);
 #ifdef COT_PHASE_STATS
-    const int ntested = __popc(__ballot_sync(FULLMASK, jl >= 0));  // warp-wide, outside the lane-0 branch
+    const int ntested = __popc(W.ballot(jl >= 0));  // segment-wide, outside the lane-0 branch
     PSTAT_ADD(4, ntested);
 #endif
     if (have == 0u) return P;
     int ord = lane;
     if (nearest && __popc(have) > 1) {
         double k2 = cut ? key : INFINITY;
-        warp_sort(k2, ord, lane);
-        have = lanes_below(__popc(have));
+        warp_sort<LPC>(k2, ord, lane);
+        have = W.below(__popc(have));
     } else {
         nearest = false;
     }
     while (have != 0u && P.nv > 0) {
         const int t = __ffs(have) - 1;
         have &= have - 1u;
-        const int src = nearest ? __shfl_sync(FULLMASK, ord, t) : t;
-        const int j = __shfl_sync(FULLMASK, jl, src);
-        const double a = __shfl_sync(FULLMASK, al, src);
-        const double b = __shfl_sync(FULLMASK, bl, src);
-        const double c = __shfl_sync(FULLMASK, cl, src);
+        const int src = nearest ? W.shfl(ord, t) : t;
+        const int j = W.shfl(jl, src);
+        const double a = W.shfl(al, src);
+        const double b = W.shfl(bl, src);
+        const double c = W.shfl(cl, src);
         const int before = P.nv;
-        if (!rclip(P, a, b, c, j, lane, S)) {
+        if (!rclip<LPC>(P, a, b, c, j, lane, S)) {
             P.nv = -1;
             return P;
         }
@@ -1096,11 +1171,13 @@ __device__ __noinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 *__
 // line pair, same symmetric meet).  Otherwise the result has nv = -2 and
 // the caller clips.  Cuts by sites outside the list are found by the
 // certificate; cuts by domain sides outside it are applied here (nv = -1:
-// the ring grew past 32 vertices).
-__device__ __noinline__ RegPoly ring_from_cache(int lab, int m, const double2 *__restrict__ sxy, double4 box,
+// the ring grew past LPC vertices).
+template <int LPC>
+__device__ __forceinline__ RegPoly ring_from_cache(int lab, int m, const double2 *__restrict__ sxy, double4 box,
                                                 double2 si, double wi, const double *__restrict__ wt, int lane,
                                                 FastScratch &S)
 {
+    const Seg<LPC> W;
     RegPoly P;
     const bool act = lane < m;
     double la = 0.0, lb = 0.0, lc = 0.0, key;
@@ -1110,25 +1187,25 @@ __device__ __noinline__ RegPoly ring_from_cache(int lab, int m, const double2 *_
     }
     const int pv = act ? (lane == 0 ? m - 1 : lane - 1) : lane;
     const int nx = act ? (lane + 1 == m ? 0 : lane + 1) : lane;
-    const double pa = __shfl_sync(FULLMASK, la, pv), pb = __shfl_sync(FULLMASK, lb, pv);
-    const double pc = __shfl_sync(FULLMASK, lc, pv);
+    const double pa = W.shfl(la, pv), pb = W.shfl(lb, pv);
+    const double pc = W.shfl(lc, pv);
     double vx = 0.0, vy = 0.0;
     bool ok = true;
     if (act) ok = line_meet(pa, pb, pc, la, lb, lc, vx, vy);
     for (int j = 0; j < m; j++) {
-        const double ja = __shfl_sync(FULLMASK, la, j), jb = __shfl_sync(FULLMASK, lb, j);
-        const double jc = __shfl_sync(FULLMASK, lc, j);
+        const double ja = W.shfl(la, j), jb = W.shfl(lb, j);
+        const double jc = W.shfl(lc, j);
         if (act && j != lane && j != pv && side(ja, jb, jc, vx, vy) > 0.0) ok = false;
     }
-    const double nvx = __shfl_sync(FULLMASK, vx, nx), nvy = __shfl_sync(FULLMASK, vy, nx);
-    const double na = __shfl_sync(FULLMASK, la, nx), nb = __shfl_sync(FULLMASK, lb, nx);
+    const double nvx = W.shfl(vx, nx), nvy = W.shfl(vy, nx);
+    const double na = W.shfl(la, nx), nb = W.shfl(lb, nx);
     if (act) {
         // edge k runs along (-b, a) from vertex k to vertex k+1
         const double len = __fma_rn(nvx - vx, -lb, __dmul_rn(nvy - vy, la));
         const double turn = __fma_rn(-lb, na, __dmul_rn(la, nb));
         if (!(len > 0.0) || !(turn > 0.0)) ok = false;
     }
-    if (!__all_sync(FULLMASK, ok)) {
+    if (!W.all(ok)) {
         P.nv = -2;
         return P;
     }
@@ -1144,8 +1221,8 @@ __device__ __noinline__ RegPoly ring_from_cache(int lab, int m, const double2 *_
         double a, b, c;
         side_line(k, box, a, b, c);
         const bool out = lane < P.nv && side(a, b, c, P.x, P.y) > 0.0;
-        if (__any_sync(FULLMASK, out)) {
-            if (!rclip(P, a, b, c, -(k + 1), lane, S)) {
+        if (W.any(out)) {
+            if (!rclip<LPC>(P, a, b, c, -(k + 1), lane, S)) {
                 P.nv = -1;
                 return P;
             }
@@ -1155,322 +1232,347 @@ __device__ __noinline__ RegPoly ring_from_cache(int lab, int m, const double2 *_
 }
 
 // Sites of `cnt[k]` consecutive ranges starting at `st[k]` (k = lane, up to
-// 32 ranges), applied in chunks of 32.  inc = inclusive scan of cnt.
-__device__ __noinline__ RegPoly apply_ranges(RegPoly P, int st, int cnt, int inc, int self, const double2 *__restrict__ sxy,
+// LPC ranges), applied in chunks of LPC.  inc = inclusive scan of cnt.
+template <int LPC>
+__device__ __forceinline__ RegPoly apply_ranges(RegPoly P, int st, int cnt, int inc, int self, const double2 *__restrict__ sxy,
                                              double2 si, double wi, const double *__restrict__ wt, int lane,
                                              FastScratch &S, bool nearest)
 {
-    const int tot = __shfl_sync(FULLMASK, inc, 31);
-    for (int base = 0; base < tot && P.nv > 0; base += 32) {
+    const Seg<LPC> W;
+    const int tot = W.shfl(inc, LPC - 1);
+    for (int base = 0; base < tot && P.nv > 0; base += LPC) {
         const int t = base + lane;
         // k = number of ranges that end at or before t
         int k = 0;
 #pragma unroll
-        for (int sft = 16; sft >= 1; sft >>= 1) {
-            int v = __shfl_sync(FULLMASK, inc, k + sft - 1);
+        for (int sft = LPC / 2; sft >= 1; sft >>= 1) {
+            int v = W.shfl(inc, k + sft - 1);
             if (v <= t) k += sft;
         }
-        const int ik = __shfl_sync(FULLMASK, inc, k & 31);
-        const int sk = __shfl_sync(FULLMASK, st, k & 31);
-        const int ck = __shfl_sync(FULLMASK, cnt, k & 31);
+        const int ik = W.shfl(inc, k & (LPC - 1));
+        const int sk = W.shfl(st, k & (LPC - 1));
+        const int ck = W.shfl(cnt, k & (LPC - 1));
         int j = (t < tot) ? sk + (t - (ik - ck)) : -1;
         if (j == self) j = -1;
-        P = apply_chunk(P, j, sxy, si, wi, wt, lane, S, nearest);
+        P = apply_chunk<LPC>(P, j, sxy, si, wi, wt, lane, S, nearest);
         if (P.nv < 0) return P;
     }
     return P;
 }
 
+// One cell, worked by one segment of LPC lanes (lane = index in the segment).
 // EXACT = true: the per-pixel path that also yields centroids (with the
-// reference's 1e-10 piece rule) and the render; false: the solver's hot path
-// (masses and objective only), which keeps the kernel's code small.
-template <int MINB, bool EXACT>
-__global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
+// reference's 1e-10 piece rule) and the render, a whole warp per cell;
+// false: the solver's hot path (masses and objective only).  Rings that
+// outgrow LPC vertices go to olist / ocount for the next pass.
+template <bool EXACT, int LPC>
+__device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, const int i, FastScratch &S,
+                                          int *olist, int *ocount)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[wib];
+    const Seg<LPC> SG;
+    const int lane = SG.sl;
     const double *__restrict__ wt = a.wt;
-    PSTAT_INIT();
-
-    while (true) {
-        int idx = 0;
-        if (lane == 0) idx = atomicAdd(a.work, 1);
-        idx = __shfl_sync(FULLMASK, idx, 0);
-        if (idx >= g.n) break;
-        const int i = idx;
-        const double2 si = g.xy[i];
-        const double wi = wt[i];
-        PSTAT_CLOCK(t0);
-        // domain rectangle, CCW, relative to the site
-        RegPoly P;
-        P.nv = 4;
-        {
-            const double x0 = g.pd[0] - si.x, x1 = g.pd[1] - si.x, y0 = g.pd[2] - si.y, y1 = g.pd[3] - si.y;
-            P.x = (lane == 1 || lane == 2) ? x1 : x0;
-            P.y = (lane >= 2) ? y1 : y0;
-            P.a = lane == 1 ? 1.0 : (lane == 3 ? -1.0 : 0.0);
-            P.b = lane == 0 ? -1.0 : (lane == 2 ? 1.0 : 0.0);
-            P.c = lane == 0 ? -y0 : (lane == 1 ? x1 : (lane == 2 ? y1 : -x0));
-            P.l = -(lane + 1);
-        }
-        bool ok = true;
-        if (lane == 0) S.kn = -1;
-        __syncwarp();
-        const int bi = g.sbucket[i];
-        const int bu = bi % g.bx, bv = bi / g.bx;
-        // ---- 1. first candidates: last evaluation's ring or neighbours, else
-        //         the 3x3 buckets around the site, nearest first ---------------
-        // cache: +m = the ring's m generators in order (domain sides
-        // included), -m = m sites in no order (long rings), hidden cells
-        // -(COT_NB_HIDDEN + m)
-        const int nraw = (a.nbn != nullptr) ? a.nbn[i] : 0;
-        const bool hidden = nraw < -COT_NB_HIDDEN;
-        const int ncache = min(nraw >= 0 ? nraw : (hidden ? -nraw - COT_NB_HIDDEN : -nraw), COT_NBC);
-        bool cached = ncache > 0;
-        if (cached) {
-            const int lab = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
-            bool direct = false;
-            if (nraw >= 3) {
-                const double4 box = make_double4(g.pd[0] - si.x, g.pd[1] - si.x, g.pd[2] - si.y, g.pd[3] - si.y);
-                const RegPoly Q = ring_from_cache(lab, ncache, g.xy, box, si, wi, wt, lane, S);
-                if (Q.nv != -2) {
-                    P = Q;
-                    direct = true;
-                }
-            }
-            PSTAT_ADD(12, direct ? 1 : 0);
-            if (!direct) {
-                const int j = (lane < ncache && lab >= 0) ? lab : -1;
-                P = apply_chunk(P, j, g.xy, si, wi, wt, lane, S, false);
-            }
-            // a hidden cell that reappears gets the window as well, so that
-            // the certificate starts from a tight ring
-            if (hidden && P.nv > 0) cached = false;
-        }
-        if (!cached && P.nv > 0) {
-            int bcnt = 0, bst = 0;
-            if (lane < 9) {
-                const int du = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
-                const int dv = (lane == 3 || lane == 5 || lane == 6) ? 1 : (lane == 4 || lane == 7 || lane == 8) ? -1 : 0;
-                const int u = bu + du, v = bv + dv;
-                if (u >= 0 && u < g.bx && v >= 0 && v < g.by) {
-                    const int b = u + v * g.bx;
-                    bst = g.bstart[b];
-                    bcnt = g.bstart[b + 1] - bst;
-                }
-            }
-            const int inc = warp_incl_scan(bcnt, lane);
-            P = apply_ranges(P, bst, bcnt, inc, i, g.xy, si, wi, wt, lane, S, true);
-        }
-        ok = P.nv >= 0;
-        const int win = cached ? -1 : COT_WIN;
-        PSTAT_CLOCK(t1);
-        PSTAT_ADD(0, t1 - t0);
-        PSTAT_ADD(10, cached ? 1 : 0);
-        // ---- 2. certificate over the bound tree --------------------------------
-        const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
-        bool brute = false;
-        if (ok && P.nv > 0 && g.nlev > 0) {
-            if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
-            __syncwarp();
-            const int nv0 = P.nv;
-            const int top = g.nlev - 1;
-            int ncur = g.lev_w[top] * g.lev_h[top];
-            if (ncur > COT_FRMAX) brute = true;
-            int cur = 0;
-            if (!brute) {
-                // frontier entries are packed node coordinates u | v << 16
-                const int tw = g.lev_w[top];
-                for (int q = lane; q < ncur; q += 32) S.fr[0][q] = (q % tw) | ((q / tw) << 16);
-                __syncwarp();
-            }
-            for (int L = top; L >= 0 && !brute; L--) {
-                int nnext = 0;
-                const int off = g.lev_off[L], W = g.lev_w[L];
-                PSTAT_ADD(7, ncur);
-                for (int base = 0; base < ncur; base += 32) {
-                    const int q = (base + lane < ncur) ? S.fr[cur][base + lane] : -1;
-                    bool keep = false;
-                    int u = 0, v = 0;
-                    if (q >= 0) {
-                        u = q & 0xffff;
-                        v = q >> 16;
-                        const bool inwin = L == 0 && abs(u - bu) <= win && abs(v - bv) <= win;
-                        keep = !inwin && !node_excluded(S, nv0, g, off + u + v * W, si, halfs2w);
-                    }
-                    if (L == 0) {
-                        const unsigned m = __ballot_sync(FULLMASK, keep);
-                        const int cnt = __popc(m);
-                        if (nnext + cnt > COT_FRMAX) { brute = true; break; }
-                        if (keep) S.fr[1 - cur][nnext + __popc(m & ((1u << lane) - 1u))] = u + v * W;
-                        nnext += cnt;
-                    } else {
-                        const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1];
-                        int chc = 0;
-                        if (keep) {
-                            chc = (2 * u + 1 < cw ? 2 : 1) * (2 * v + 1 < ch ? 2 : 1);
-                        }
-                        const int inc = warp_incl_scan(chc, lane);
-                        const int cnt = __shfl_sync(FULLMASK, inc, 31);
-                        if (nnext + cnt > COT_FRMAX) { brute = true; break; }
-                        int pos = nnext + inc - chc;
-                        if (keep) {
-                            for (int bb = 0; bb < 2; bb++)
-                                for (int aa = 0; aa < 2; aa++)
-                                    if (2 * u + aa < cw && 2 * v + bb < ch) S.fr[1 - cur][pos++] = (2 * u + aa) | ((2 * v + bb) << 16);
-                        }
-                        nnext += cnt;
-                    }
-                }
-                __syncwarp();
-                if (brute) break;
-                cur = 1 - cur;
-                ncur = nnext;
-            }
-            if (!brute && ncur > 0) {
-                // sites of every surviving leaf, 32 leaves at a time
-                PSTAT_ADD(5, ncur);
-                for (int lb = 0; lb < ncur && ok && P.nv > 0; lb += 32) {
-                    int st = 0, cnt = 0;
-                    if (lb + lane < ncur) {
-                        const int b = S.fr[cur][lb + lane];
-                        st = g.bstart[b];
-                        cnt = g.bstart[b + 1] - st;
-                    }
-                    const int inc = warp_incl_scan(cnt, lane);
-                    P = apply_ranges(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
-                    ok = P.nv >= 0;
-                }
+    const double2 si = g.xy[i];
+    const double wi = wt[i];
+    PSTAT_CLOCK(t0);
+    // domain rectangle, CCW, relative to the site
+    RegPoly P;
+    P.nv = 4;
+    {
+        const double x0 = g.pd[0] - si.x, x1 = g.pd[1] - si.x, y0 = g.pd[2] - si.y, y1 = g.pd[3] - si.y;
+        P.x = (lane == 1 || lane == 2) ? x1 : x0;
+        P.y = (lane >= 2) ? y1 : y0;
+        P.a = lane == 1 ? 1.0 : (lane == 3 ? -1.0 : 0.0);
+        P.b = lane == 0 ? -1.0 : (lane == 2 ? 1.0 : 0.0);
+        P.c = lane == 0 ? -y0 : (lane == 1 ? x1 : (lane == 2 ? y1 : -x0));
+        P.l = -(lane + 1);
+    }
+    bool ok = true;
+    if (lane == 0) S.kn = -1;
+    SG.sync();
+    const int bi = g.sbucket[i];
+    const int bu = bi % g.bx, bv = bi / g.bx;
+    // ---- 1. first candidates: last evaluation's ring or neighbours, else
+    //         the 3x3 buckets around the site, nearest first ---------------
+    // cache: +m = the ring's m generators in order (domain sides
+    // included), -m = m sites in no order (long rings), hidden cells
+    // -(COT_NB_HIDDEN + m)
+    const int nraw = (a.nbn != nullptr) ? a.nbn[i] : 0;
+    const bool hidden = nraw < -COT_NB_HIDDEN;
+    const int ncache = min(nraw >= 0 ? nraw : (hidden ? -nraw - COT_NB_HIDDEN : -nraw), COT_NBC);
+    bool cached = ncache > 0;
+    if (cached) {
+        const int lab = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
+        bool direct = false;
+        if (nraw >= 3) {
+            const double4 box = make_double4(g.pd[0] - si.x, g.pd[1] - si.x, g.pd[2] - si.y, g.pd[3] - si.y);
+            const RegPoly Q = ring_from_cache<LPC>(lab, ncache, g.xy, box, si, wi, wt, lane, S);
+            if (Q.nv != -2) {
+                P = Q;
+                direct = true;
             }
         }
-        PSTAT_ADD(9, brute ? 1 : 0);
-        if (ok && brute && P.nv > 0) {
-            // frontier overflow: test every bucket against the current ring
-            const int nb = g.bx * g.by;
-            for (int base = 0; base < nb && ok && P.nv > 0; base += 32) {
-                if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
-                __syncwarp();
-                const int b = base + lane;
+        PSTAT_ADD(12, direct ? 1 : 0);
+        if (!direct) {
+            const int j = (lane < ncache && lab >= 0) ? lab : -1;
+            P = apply_chunk<LPC>(P, j, g.xy, si, wi, wt, lane, S, false);
+        }
+        // a hidden cell that reappears gets the window as well, so that
+        // the certificate starts from a tight ring
+        if (hidden && P.nv > 0) cached = false;
+    }
+    if (!cached && P.nv > 0) {
+        int bcnt = 0, bst = 0;
+        if (lane < 9) {
+            const int du = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
+            const int dv = (lane == 3 || lane == 5 || lane == 6) ? 1 : (lane == 4 || lane == 7 || lane == 8) ? -1 : 0;
+            const int u = bu + du, v = bv + dv;
+            if (u >= 0 && u < g.bx && v >= 0 && v < g.by) {
+                const int b = u + v * g.bx;
+                bst = g.bstart[b];
+                bcnt = g.bstart[b + 1] - bst;
+            }
+        }
+        const int inc = SG.incl_scan(bcnt);
+        P = apply_ranges<LPC>(P, bst, bcnt, inc, i, g.xy, si, wi, wt, lane, S, true);
+    }
+    ok = P.nv >= 0;
+    const int win = cached ? -1 : COT_WIN;
+    PSTAT_CLOCK(t1);
+    PSTAT_ADD(0, t1 - t0);
+    PSTAT_ADD(10, cached ? 1 : 0);
+    // ---- 2. certificate over the bound tree --------------------------------
+    const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
+    bool brute = false;
+    if (ok && P.nv > 0 && g.nlev > 0) {
+        if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+        SG.sync();
+        const int nv0 = P.nv;
+        // start at the deepest level that still fits one round of lanes:
+        // every node there is tested, a superset of what the levels above
+        // would keep, without their rounds
+        int top = g.nlev - 1;
+        while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= LPC) top--;
+        int ncur = g.lev_w[top] * g.lev_h[top];
+        if (ncur > COT_FRMAX) brute = true;
+        int cur = 0;
+        if (!brute) {
+            // frontier entries are packed node coordinates u | v << 16
+            const int tw = g.lev_w[top];
+            for (int q = lane; q < ncur; q += LPC) S.fr[0][q] = (q % tw) | ((q / tw) << 16);
+            SG.sync();
+        }
+        for (int L = top; L >= 0 && !brute; L--) {
+            int nnext = 0;
+            const int off = g.lev_off[L], W = g.lev_w[L];
+            PSTAT_ADD(7, ncur);
+            for (int base = 0; base < ncur; base += LPC) {
+                const int q = (base + lane < ncur) ? S.fr[cur][base + lane] : -1;
                 bool keep = false;
-                if (b < nb) {
-                    const int u = b % g.bx, v = b / g.bx;
-                    const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
-                    keep = !inwin && !node_excluded(S, P.nv, g, b, si, halfs2w);
+                int u = 0, v = 0;
+                if (q >= 0) {
+                    u = q & 0xffff;
+                    v = q >> 16;
+                    const bool inwin = L == 0 && abs(u - bu) <= win && abs(v - bv) <= win;
+                    keep = !inwin && !node_excluded(S, nv0, g, off + u + v * W, si, halfs2w);
                 }
-                __syncwarp();
+                if (L == 0) {
+                    const unsigned m = SG.ballot(keep);
+                    const int cnt = __popc(m);
+                    if (nnext + cnt > COT_FRMAX) { brute = true; break; }
+                    if (keep) S.fr[1 - cur][nnext + __popc(m & ((1u << lane) - 1u))] = u + v * W;
+                    nnext += cnt;
+                } else {
+                    const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1];
+                    int chc = 0;
+                    if (keep) {
+                        chc = (2 * u + 1 < cw ? 2 : 1) * (2 * v + 1 < ch ? 2 : 1);
+                    }
+                    const int inc = SG.incl_scan(chc);
+                    const int cnt = SG.shfl(inc, LPC - 1);
+                    if (nnext + cnt > COT_FRMAX) { brute = true; break; }
+                    int pos = nnext + inc - chc;
+                    if (keep) {
+                        for (int bb = 0; bb < 2; bb++)
+                            for (int aa = 0; aa < 2; aa++)
+                                if (2 * u + aa < cw && 2 * v + bb < ch) S.fr[1 - cur][pos++] = (2 * u + aa) | ((2 * v + bb) << 16);
+                    }
+                    nnext += cnt;
+                }
+            }
+            SG.sync();
+            if (brute) break;
+            cur = 1 - cur;
+            ncur = nnext;
+        }
+        if (!brute && ncur > 0) {
+            // sites of every surviving leaf, LPC leaves at a time
+            PSTAT_ADD(5, ncur);
+            for (int lb = 0; lb < ncur && ok && P.nv > 0; lb += LPC) {
                 int st = 0, cnt = 0;
-                if (keep) {
+                if (lb + lane < ncur) {
+                    const int b = S.fr[cur][lb + lane];
                     st = g.bstart[b];
                     cnt = g.bstart[b + 1] - st;
                 }
-                const int inc = warp_incl_scan(cnt, lane);
-                P = apply_ranges(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
+                const int inc = SG.incl_scan(cnt);
+                P = apply_ranges<LPC>(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
                 ok = P.nv >= 0;
             }
         }
-        if (!ok) {
-            // ring above 32 vertices: hand the cell to the large-capacity pass
-            if (lane == 0) {
-                const int slot = atomicAdd(a.ovf_count, 1);
-                a.ovf_list[slot] = i;
-                a.nv[i] = 33;
+    }
+    PSTAT_ADD(9, brute ? 1 : 0);
+    if (ok && brute && P.nv > 0) {
+        // frontier overflow: test every bucket against the current ring
+        const int nb = g.bx * g.by;
+        for (int base = 0; base < nb && ok && P.nv > 0; base += LPC) {
+            if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+            SG.sync();
+            const int b = base + lane;
+            bool keep = false;
+            if (b < nb) {
+                const int u = b % g.bx, v = b / g.bx;
+                const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
+                keep = !inwin && !node_excluded(S, P.nv, g, b, si, halfs2w);
             }
-            __syncwarp();
-            continue;
-        }
-        // ---- 3. integrate the density over the cell --------------------------
-        PSTAT_CLOCK(t2);
-        PSTAT_ADD(1, t2 - t1);
-        const int nv = P.nv;
-        if (nv >= 3) {
-            // canonical ring start (smallest edge generator) so the integration
-            // sums in the same order whatever order the clips came in
-            const int key = lane < nv ? P.l : 0x7fffffff;
-            const int mn = __reduce_min_sync(FULLMASK, key);
-            const int r = __ffs(__ballot_sync(FULLMASK, key == mn)) - 1;
-            int src = lane + r;
-            if (src >= nv) src -= nv;
-            P.x = __shfl_sync(FULLMASK, P.x, src);
-            P.y = __shfl_sync(FULLMASK, P.y, src);
-            P.a = __shfl_sync(FULLMASK, P.a, src);
-            P.b = __shfl_sync(FULLMASK, P.b, src);
-            P.c = __shfl_sync(FULLMASK, P.c, src);
-            P.l = __shfl_sync(FULLMASK, P.l, src);
-        }
-        if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
-        __syncwarp();
-        CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (nv >= 3) {
-            if constexpr (EXACT)
-                acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
-            else
-                acc = integrate_fast(S, nv, pix_geo(g), si, lane);
-        }
-        PSTAT_CLOCK(t3);
-        PSTAT_ADD(2, t3 - t2);
-        PSTAT_ADD(8, 1);
-        PSTAT_ADD(11, nv);
-        double pcx = 0.0, pcy = 0.0;
-        if constexpr (EXACT) {
-            if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid(S, nv, lane, pcx, pcy);
-        }
-        if (a.ring_xy != nullptr && lane < nv && lane < a.ring_cap) {
-            a.ring_xy[2 * ((size_t)i * a.ring_cap + lane)] = si.x + P.x;
-            a.ring_xy[2 * ((size_t)i * a.ring_cap + lane) + 1] = si.y + P.y;
-            a.ring_lab[(size_t)i * a.ring_cap + lane] = P.l;
-        }
-        if constexpr (EXACT) {
-            if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(S, nv, si, a.solid_z, a.solid_light) : 0.0;
-        }
-        if (a.nbn != nullptr) {
-            // this evaluation seeds the next: a ring of up to COT_NBC edges
-            // in order (domain sides included); else its sites, or for a
-            // hidden cell the site that emptied its ring and that ring's sites
-            if (nv >= 3 && nv <= COT_NBC) {
-                if (lane < nv) a.nbc[(size_t)i * COT_NBC + lane] = P.l;
-                if (lane == 0) a.nbn[i] = nv;
-            } else {
-                int lab = lane < nv ? P.l : -1;
-                if (nv == 0) {
-                    __syncwarp();
-                    const int kn = S.kn;
-                    lab = -1;
-                    if (kn >= 0) lab = lane == 0 ? S.kill : (lane - 1 < kn ? S.KL[lane - 1] : -1);
-                }
-                const bool isn = lab >= 0;
-                const unsigned m = __ballot_sync(FULLMASK, isn);
-                const int pos = __popc(m & ((1u << lane) - 1u));
-                if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = lab;
-                const int cnt = min(__popc(m), COT_NBC);
-                if (lane == 0) a.nbn[i] = cnt == 0 ? 0 : (nv == 0 ? -(COT_NB_HIDDEN + cnt) : -cnt);
+            SG.sync();
+            int st = 0, cnt = 0;
+            if (keep) {
+                st = g.bstart[b];
+                cnt = g.bstart[b + 1] - st;
             }
+            const int inc = SG.incl_scan(cnt);
+            P = apply_ranges<LPC>(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
+            ok = P.nv >= 0;
         }
+    }
+    if (!ok) {
+        // ring above LPC vertices: hand the cell to the next pass
         if (lane == 0) {
-            a.mu[i] = acc.mu;
-            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941);
-            // stored without its -w_i nu_i term, which the reduction adds, so
-            // that nu may change after the cells are built
-            a.fc[i] = -(acc.S - wi * acc.mu);
-            a.nv[i] = nv;
-            if (a.cen != nullptr) {
-                const bool ex = nv >= 3;
-                a.exist[i] = ex ? 1 : 0;
-                double cx = si.x, cy = si.y;
-                if (ex) {
-                    if (a.weighted && acc.Mt != 0.0) {
-                        cx = si.x + acc.Mx / acc.Mt;
-                        cy = si.y + acc.My / acc.Mt;
-                    } else {
-                        cx = si.x + pcx;
-                        cy = si.y + pcy;
-                    }
-                }
-                a.cen[2 * i] = cx;
-                a.cen[2 * i + 1] = cy;
-            }
+            const int slot = atomicAdd(ocount, 1);
+            olist[slot] = i;
+            a.nv[i] = LPC + 1;
         }
+        SG.sync();
+        return;
+    }
+    // ---- 3. integrate the density over the cell --------------------------
+    PSTAT_CLOCK(t2);
+    PSTAT_ADD(1, t2 - t1);
+    const int nv = P.nv;
+    if (nv >= 3) {
+        // canonical ring start (smallest edge generator) so the integration
+        // sums in the same order whatever order the clips came in
+        const int key = lane < nv ? P.l : 0x7fffffff;
+        const int mn = SG.imin(key);
+        const int r = __ffs(SG.ballot(key == mn)) - 1;
+        int src = lane + r;
+        if (src >= nv) src -= nv;
+        P.x = SG.shfl(P.x, src);
+        P.y = SG.shfl(P.y, src);
+        P.a = SG.shfl(P.a, src);
+        P.b = SG.shfl(P.b, src);
+        P.c = SG.shfl(P.c, src);
+        P.l = SG.shfl(P.l, src);
+    }
+    if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+    SG.sync();
+    CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (nv >= 3) {
+        if constexpr (EXACT)
+            acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
+        else
+            acc = integrate_fast<LPC>(S, nv, pix_geo(g), si, lane);
+    }
+    PSTAT_CLOCK(t3);
+    PSTAT_ADD(2, t3 - t2);
+    PSTAT_ADD(8, 1);
+    PSTAT_ADD(11, nv);
+    double pcx = 0.0, pcy = 0.0;
+    if constexpr (EXACT) {
+        if (a.cen != nullptr && nv >= 3 && (!a.weighted || acc.Mt == 0.0)) poly_centroid(S, nv, lane, pcx, pcy);
+    }
+    if (a.ring_xy != nullptr && lane < nv && lane < a.ring_cap) {
+        a.ring_xy[2 * ((size_t)i * a.ring_cap + lane)] = si.x + P.x;
+        a.ring_xy[2 * ((size_t)i * a.ring_cap + lane) + 1] = si.y + P.y;
+        a.ring_lab[(size_t)i * a.ring_cap + lane] = P.l;
+    }
+    if constexpr (EXACT) {
+        if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(S, nv, si, a.solid_z, a.solid_light) : 0.0;
+    }
+    if (a.nbn != nullptr) {
+        // this evaluation seeds the next: a ring of up to COT_NBC edges
+        // in order (domain sides included); else its sites, or for a
+        // hidden cell the site that emptied its ring and that ring's sites
+        if (nv >= 3 && nv <= COT_NBC) {
+            if (lane < nv) a.nbc[(size_t)i * COT_NBC + lane] = P.l;
+            if (lane == 0) a.nbn[i] = nv;
+        } else {
+            int lab = lane < nv ? P.l : -1;
+            if (nv == 0) {
+                SG.sync();
+                const int kn = S.kn;
+                lab = -1;
+                if (kn >= 0) lab = lane == 0 ? S.kill : (lane - 1 < kn ? S.KL[lane - 1] : -1);
+            }
+            const bool isn = lab >= 0;
+            const unsigned m = SG.ballot(isn);
+            const int pos = __popc(m & ((1u << lane) - 1u));
+            if (isn && pos < COT_NBC) a.nbc[(size_t)i * COT_NBC + pos] = lab;
+            const int cnt = min(__popc(m), COT_NBC);
+            if (lane == 0) a.nbn[i] = cnt == 0 ? 0 : (nv == 0 ? -(COT_NB_HIDDEN + cnt) : -cnt);
+        }
+    }
+    if (lane == 0) {
+        a.mu[i] = acc.mu;
+        // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941);
+        // stored without its -w_i nu_i term, which the reduction adds, so
+        // that nu may change after the cells are built
+        a.fc[i] = -(acc.S - wi * acc.mu);
+        a.nv[i] = nv;
+        if (a.cen != nullptr) {
+            const bool ex = nv >= 3;
+            a.exist[i] = ex ? 1 : 0;
+            double cx = si.x, cy = si.y;
+            if (ex) {
+                if (a.weighted && acc.Mt != 0.0) {
+                    cx = si.x + acc.Mx / acc.Mt;
+                    cy = si.y + acc.My / acc.Mt;
+                } else {
+                    cx = si.x + pcx;
+                    cy = si.y + pcy;
+                }
+            }
+            a.cen[2 * i] = cx;
+            a.cen[2 * i + 1] = cy;
+        }
+    }
+}
+
+// The persistent cell kernel: each warp fetches 32 / LPC cells at a time
+// (one per segment) from a counter, so that large cells leave no tail and the
+// segments of a warp run the same phases together.  pass 0: every cell,
+// rings above LPC vertices into ovf_list; pass 1: the cells of ovf_list,
+// rings above LPC into ovf_list2.
+template <int MINB, bool EXACT, int LPC>
+__global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a, int pass)
+{
+    static_assert(!EXACT || LPC == 32, "the exact path works a whole warp per cell");
+    constexpr int CPW = 32 / LPC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x / LPC];
+    PSTAT_INIT();
+    const int total = pass == 0 ? g.n : a.ovf_count[0];
+    int *fetch = a.ovf_count + (pass == 0 ? 1 : 4);
+    int *olist = pass == 0 ? a.ovf_list : a.ovf_list2;
+    int *ocount = a.ovf_count + (pass == 0 ? 0 : 3);
+    while (true) {
+        int base = 0;
+        if ((threadIdx.x & 31) == 0) base = atomicAdd(fetch, CPW);
+        base = __shfl_sync(FULLMASK, base, 0);
+        if (base >= total) break;
+        const int slot = base + (int)(threadIdx.x & 31) / LPC;
+        if (slot < total) fast_cell<EXACT, LPC>(g, a, pass == 0 ? slot : a.ovf_list[slot], S, olist, ocount);
         __syncwarp();
     }
     PSTAT_FLUSH();
@@ -1479,11 +1581,13 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a)
 // ---------------------------------------------------------------------------
 // the cell kernel
 // ---------------------------------------------------------------------------
-// mode 0: every cell; mode 1: the cells listed in ovf_list.  Warps fetch
-// cells dynamically from a counter so that large cells do not leave a tail.
+// mode 0: every cell; mode 1: the cells listed in ovf_list; mode 2: those in
+// ovf_list2.  Warps fetch cells dynamically from a counter so that large cells
+// do not leave a tail.
 template <int MAXV, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int mode)
 {
+    PSTAT_LPC32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -1491,13 +1595,17 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
     const double *__restrict__ wt = a.wt;
     PSTAT_INIT();
 
-    const int total = (mode == 0) ? g.n : *a.ovf_count;
+    // counters: [0] ovf_list size, [1] pass-0 fetch, [2] mode-1 fetch,
+    // [3] ovf_list2 size, [4] second-pass fetch, [5] mode-2 fetch
+    const int total = (mode == 0) ? g.n : a.ovf_count[mode == 1 ? 0 : 3];
+    int *fetch = a.ovf_count + (mode == 0 ? 1 : (mode == 1 ? 2 : 5));
+    const int *list = mode == 1 ? a.ovf_list : a.ovf_list2;
     while (true) {
         int idx = 0;
-        if (lane == 0) idx = atomicAdd(a.work + mode, 1);
+        if (lane == 0) idx = atomicAdd(fetch, 1);
         idx = __shfl_sync(FULLMASK, idx, 0);
         if (idx >= total) break;
-        const int i = (mode == 0) ? idx : a.ovf_list[idx];
+        const int i = (mode == 0) ? idx : list[idx];
         const double2 si = g.xy[i];
         const double wi = wt[i];
         int status = 0;
@@ -1563,6 +1671,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
         bool brute = false;
         if (nv > 0 && status == 0 && g.nlev > 0) {
             int top = g.nlev - 1;
+            while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= 32) top--;
             int ncur = g.lev_w[top] * g.lev_h[top];
             if (ncur > COT_FRMAX) brute = true;
             int cur = 0;
@@ -1740,12 +1849,22 @@ static size_t cells_smem(int maxv, int warps)
 }
 
 #define CELLS_WPB 4
-#define CELLS_MINB 4
-static int g_cells_blocks_per_sm = 0;
+#define CELLS_MINB 5
+static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0;
 
-void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms, CotCtx &c)
+template <bool EXACT, int LPC>
+static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int blocks, cudaStream_t s)
 {
-    (void)warps_per_block;
+    const size_t sm = sizeof(FastScratch) * CELLS_WPB * (32 / LPC);
+    k_cells_fast<CELLS_MINB, EXACT, LPC><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a, pass);
+}
+
+// One evaluation: bucket and tree bounds, then the cells.  cells_per_warp 2
+// runs the hot path on 16-lane segments (two cells per warp) with a 32-lane
+// second pass for rings above 16 vertices; every path ends with the
+// 256-vertex pass for rings above 32.
+void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms, CotCtx &c)
+{
     cudaStream_t s = c.s;
     int nb = g.bx * g.by;
     k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar);
@@ -1756,25 +1875,33 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int n
         k_tree_level<<<(cnt + 127) / 128, 128, 0, s>>>(g, L);
         c.launches++;
     }
-    // ovf_count and the two work counters are contiguous
-    cudaMemsetAsync(a.ovf_count, 0, 3 * sizeof(int), s);
-    int sms = num_sms > 0 ? num_sms : 148;
-    int per_sm = g_cells_blocks_per_sm > 0 ? g_cells_blocks_per_sm : CELLS_MINB;
-    int want = (g.n + CELLS_WPB - 1) / CELLS_WPB;
-    int blocks = std::min(want, sms * per_sm);
-    size_t sm = sizeof(FastScratch) * CELLS_WPB;
+    // the overflow list sizes and fetch counters
+    cudaMemsetAsync(a.ovf_count, 0, 6 * sizeof(int), s);
+    const int sms = num_sms > 0 ? num_sms : 148;
+    const bool exact = a.cen != nullptr || a.splat != nullptr || a.solid != nullptr;
+    const int lpc = (exact || cells_per_warp < 2) ? 32 : 16;
+    const int per_sm32 = g_blocks_per_sm32 > 0 ? g_blocks_per_sm32 : CELLS_MINB;
+    const int per_sm16 = g_blocks_per_sm16 > 0 ? g_blocks_per_sm16 : CELLS_MINB;
+    const int cells_per_block = CELLS_WPB * (32 / lpc);
+    const int want = (g.n + cells_per_block - 1) / cells_per_block;
+    const int blocks = std::min(want, sms * (lpc == 32 ? per_sm32 : per_sm16));
     bool timed = c.profile && c.ev != nullptr && c.ev_used + 2 <= c.ev_cap;
     if (timed) cudaEventRecord(c.ev[c.ev_used], s);
-    if (a.cen != nullptr || a.splat != nullptr || a.solid != nullptr)
-        k_cells_fast<CELLS_MINB, true><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a);
-    else
-        k_cells_fast<CELLS_MINB, false><<<blocks, 32 * CELLS_WPB, sm, s>>>(g, a);
+    if (exact) {
+        launch_fast<true, 32>(g, a, 0, blocks, s);
+    } else if (lpc == 32) {
+        launch_fast<false, 32>(g, a, 0, blocks, s);
+    } else {
+        launch_fast<false, 16>(g, a, 0, blocks, s);
+        launch_fast<false, 32>(g, a, 1, sms, s);
+        c.launches++;
+    }
     if (timed) {
         cudaEventRecord(c.ev[c.ev_used + 1], s);
         c.ev_used += 2;
     }
     // cells above 32 vertices (rare): one warp per block, 256-vertex rings
-    k_cells<256, 1><<<sms, 32, cells_smem(256, 1), s>>>(g, a, 1);
+    k_cells<256, 1><<<sms, 32, cells_smem(256, 1), s>>>(g, a, lpc == 32 ? 1 : 2);
     c.launches += 2;
     c.cell_launches += 1;
     c.evaluations += 1;
@@ -1795,15 +1922,19 @@ extern "C" __attribute__((visibility("default"))) int cot_debug_phase_stats(unsi
 
 void configure_cells_kernels()
 {
-    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(sizeof(FastScratch) * CELLS_WPB));
-    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(sizeof(FastScratch) * CELLS_WPB));
+    const int sm32 = (int)(sizeof(FastScratch) * CELLS_WPB), sm16 = 2 * sm32;
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm16);
     cudaFuncSetAttribute(k_cells<256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(256, 1));
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false>, 32 * CELLS_WPB,
-                                                      sizeof(FastScratch) * CELLS_WPB) == cudaSuccess && nb > 0)
-        g_cells_blocks_per_sm = nb;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false, 32>, 32 * CELLS_WPB,
+                                                      sm32) == cudaSuccess && nb > 0)
+        g_blocks_per_sm32 = nb;
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false, 16>, 32 * CELLS_WPB,
+                                                      sm16) == cudaSuccess && nb > 0)
+        g_blocks_per_sm16 = nb;
 }
 
 }  // namespace cot

@@ -129,9 +129,12 @@ struct CellsArgs {
     double *mu;            // per cell mass out
     double *fc;            // per cell objective out, without its -w_i nu_i term
     int *nv;               // per cell ring size out
-    int *ovf_list;         // cells to redo with the large ring capacity
-    int *ovf_count;        // device counters: [0] overflow count, [1..2] work
-    int *work;             // = ovf_count + 1
+    int *ovf_list;         // cells whose ring outgrew the first pass
+    int *ovf_list2;        // cells whose ring outgrew the second pass
+    int *ovf_count;        // 6 device counters: [0] ovf_list size, [1] first-pass
+                           // fetch, [2] large-ring fetch over ovf_list, [3]
+                           // ovf_list2 size, [4] second-pass fetch, [5]
+                           // large-ring fetch over ovf_list2
     int *nbc;              // cached neighbours, COT_NBC per cell (nullable)
     int *nbn;              // their count per cell (0: none)
     double *cen;           // centroids (nullable)
@@ -147,7 +150,7 @@ struct CellsArgs {
     int ring_cap;
 };
 
-void launch_eval(const CotGeo &g, const CellsArgs &a, int warps_per_block, int num_sms,
+void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms,
                  CotCtx &c);
 void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const int *nv,
                    const double *wt, const double *d, int max_ring, double *partials,

@@ -360,3 +360,43 @@ def test_graph_loop_matches_host_loop(gpu, mode):
     wg2, sg2 = solver_for(p).solve(np.zeros(p.n), mode=mode, tol=1e-12, history=7, max_iter=37, use_graph=0)
     wh2, sh2 = solver_for(p).solve(np.zeros(p.n), mode=mode, tol=1e-12, history=7, max_iter=37, use_graph=-1)
     assert sg2.iterations == sh2.iterations == 37 and np.array_equal(wg2, wh2)
+
+
+def test_two_cells_per_warp_parity(gpu):
+    """16-lane segments (two cells per warp): rings above 16 vertices go to a
+    32-lane pass and rings above 32 to the 256-vertex pass; a few heavy
+    sites make giant cells so that every pass runs."""
+    p = problems.make(1, g=32, res=128, beam=True)
+    rng = np.random.default_rng(23)
+    w = rng.normal(0, 0.3 / p.n, p.n)
+    # five heavy sites spread over the domain: their cells spread over a few
+    # pitches and keep most of the cells around them (rings of 16 to 40)
+    order = np.argsort(p.xy[:, 0] * 7 + p.xy[:, 1])
+    heavy = order[[150, 500, 850, 300, 700]]
+    w[heavy[:3]] += 15.0 / p.n
+    w[heavy[3:]] += 40.0 / p.n
+    one = solver_for(p, cells_per_warp=1)
+    two = solver_for(p, cells_per_warp=2)
+    off, _, _ = two.cells(w)
+    ring = np.diff(off)
+    assert (ring > 16).sum() >= 3 and (ring > 32).sum() >= 2
+    for _ in range(2):              # cold, then from the neighbour cache
+        check_eval(p, w, two)
+        f1, mu1, _, _ = one.eval(w)
+        f2, mu2, _, _ = two.eval(w)
+        assert np.abs(mu1 - mu2).max() <= 1e-13 * mu1.max()
+    with pytest.raises(capi.CotError):
+        capi.Solver(cells_per_warp=3)
+
+
+def test_two_cells_per_warp_solve(gpu):
+    p = problems.make(1, g=24, res=96, beam=True)
+    w1, s1 = solver_for(p, cells_per_warp=1).solve(np.zeros(p.n), mode=capi.SOLVE_WOLFE, tol=1e-4, history=10)
+    w2, s2 = solver_for(p, cells_per_warp=2).solve(np.zeros(p.n), mode=capi.SOLVE_WOLFE, tol=1e-4, history=10)
+    assert s1.converged and s2.converged
+    assert abs(s1.iterations - s2.iterations) <= max(3, s1.iterations // 20)
+    # the 16-lane integration sums in another order: the trajectories part by
+    # rounding, and both end inside the 1e-4 mass tolerance
+    for w in (w1, w2):
+        assert O.max_rel_error(O.evaluate(oracle_problem(p), w).mu, p.nu) <= 1e-4
+    assert np.abs(w1 - w2).max() < 1e-4 * np.abs(w1).max()
