@@ -1162,6 +1162,26 @@ __device__ __forceinline__ RegPoly apply_chunk(RegPoly P, int jl, const double2 
     return P;
 }
 
+// Clip by the domain sides that the ring crosses (nv = -1: the ring grew past
+// LPC vertices).  Rarely needed, so kept out of line.
+template <int LPC>
+__device__ __noinline__ RegPoly clip_sides(RegPoly P, double4 box, int lane, FastScratch &S)
+{
+    const Seg<LPC> W;
+    for (int k = 0; k < 4 && P.nv > 0; k++) {
+        double a, b, c;
+        side_line(k, box, a, b, c);
+        const bool out = lane < P.nv && side(a, b, c, P.x, P.y) > 0.0;
+        if (W.any(out)) {
+            if (!rclip<LPC>(P, a, b, c, -(k + 1), lane, S)) {
+                P.nv = -1;
+                return P;
+            }
+        }
+    }
+    return P;
+}
+
 // The ring of the last evaluation, rebuilt in one step: lane k < m holds the
 // generator `lab` of edge k (a site, or -1..-4 for a domain side), vertex k
 // is where the lines of edges k-1 and k meet.  Accepted only if every vertex
@@ -1216,18 +1236,10 @@ __device__ __forceinline__ RegPoly ring_from_cache(int lab, int m, const double2
     P.c = lc;
     P.l = act ? lab : 0;
     P.nv = m;
-    // domain sides that the cell now reaches
-    for (int k = 0; k < 4 && P.nv > 0; k++) {
-        double a, b, c;
-        side_line(k, box, a, b, c);
-        const bool out = lane < P.nv && side(a, b, c, P.x, P.y) > 0.0;
-        if (W.any(out)) {
-            if (!rclip<LPC>(P, a, b, c, -(k + 1), lane, S)) {
-                P.nv = -1;
-                return P;
-            }
-        }
-    }
+    // domain sides that the cell now reaches (rare: clipped out of line)
+    bool out = false;
+    if (act) out = vx < box.x || vx > box.y || vy < box.z || vy > box.w;
+    if (W.any(out)) P = clip_sides<LPC>(P, box, lane, S);
     return P;
 }
 
@@ -1258,6 +1270,26 @@ __device__ __forceinline__ RegPoly apply_ranges(RegPoly P, int st, int cnt, int 
         if (P.nv < 0) return P;
     }
     return P;
+}
+
+// Out-of-line copies for the paths a cell takes rarely once a solve runs warm
+// (no usable cache, frontier overflow): the hot path keeps one inlined copy
+// of the clip code, which keeps the kernel's working set of instructions
+// small.
+template <int LPC>
+__device__ __noinline__ RegPoly apply_ranges_cold(RegPoly P, int st, int cnt, int inc, int self,
+                                                  const double2 *__restrict__ sxy, double2 si, double wi,
+                                                  const double *__restrict__ wt, int lane, FastScratch &S, bool nearest)
+{
+    return apply_ranges<LPC>(P, st, cnt, inc, self, sxy, si, wi, wt, lane, S, nearest);
+}
+
+template <int LPC>
+__device__ __noinline__ RegPoly apply_chunk_cold(RegPoly P, int jl, const double2 *__restrict__ sxy, double2 si,
+                                                 double wi, const double *__restrict__ wt, int lane, FastScratch &S,
+                                                 bool nearest)
+{
+    return apply_chunk<LPC>(P, jl, sxy, si, wi, wt, lane, S, nearest);
 }
 
 // One cell, worked by one segment of LPC lanes (lane = index in the segment).
@@ -1315,7 +1347,7 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
         PSTAT_ADD(12, direct ? 1 : 0);
         if (!direct) {
             const int j = (lane < ncache && lab >= 0) ? lab : -1;
-            P = apply_chunk<LPC>(P, j, g.xy, si, wi, wt, lane, S, false);
+            P = apply_chunk_cold<LPC>(P, j, g.xy, si, wi, wt, lane, S, false);
         }
         // a hidden cell that reappears gets the window as well, so that
         // the certificate starts from a tight ring
@@ -1334,7 +1366,7 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
             }
         }
         const int inc = SG.incl_scan(bcnt);
-        P = apply_ranges<LPC>(P, bst, bcnt, inc, i, g.xy, si, wi, wt, lane, S, true);
+        P = apply_ranges_cold<LPC>(P, bst, bcnt, inc, i, g.xy, si, wi, wt, lane, S, true);
     }
     ok = P.nv >= 0;
     const int win = cached ? -1 : COT_WIN;
@@ -1442,7 +1474,7 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
                 cnt = g.bstart[b + 1] - st;
             }
             const int inc = SG.incl_scan(cnt);
-            P = apply_ranges<LPC>(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
+            P = apply_ranges_cold<LPC>(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
             ok = P.nv >= 0;
         }
     }
