@@ -415,11 +415,11 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.w, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.wt, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.wq, N * 8);
+    if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
     if (e == cudaSuccess) e = A((void **)&P.d, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mu, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mut, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.fc, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
     if (e == cudaSuccess) e = A((void **)&P.nv, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.ovf_list, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.ovf_list2, N * sizeof(int));
@@ -885,8 +885,7 @@ static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec,
     launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, c);
     launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, c);
     launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, c);
-    launch_reject(P.S, c);
-    launch_loop_cond(hc, P.S, c);
+    launch_reject_cond(hc, P.S, c);
     cudaGraph_t captured = nullptr;
     e = cudaStreamEndCapture(s, &captured);
     bc->launches = c.launches - saved.launches;

@@ -58,41 +58,53 @@ __shared__ unsigned long long cot_pst[16][16];
 // bucket and tree plane bounds (per evaluation)
 // ---------------------------------------------------------------------------
 
-// wt = w + t*d (t read from the device), phibar[b] = mean_j phi_j.
+// phi_j = (|s_j|^2 - w_j) / 2 at the trial point w + t d, explicitly rounded so
+// that every thread that needs a bucket's mean computes the same bits.
+__device__ __forceinline__ double trial_weight(const double *__restrict__ w, const double *__restrict__ d, double t,
+                                               int j)
+{
+    // no contraction: the trial point is w + t*d exactly as written
+    return d != nullptr ? __dadd_rn(w[j], __dmul_rn(t, d[j])) : w[j];
+}
+
+__device__ __forceinline__ double half_phi(double2 s, double wj)
+{
+    return __dmul_rn(0.5, __dsub_rn(__fma_rn(s.x, s.x, __dmul_rn(s.y, s.y)), wj));
+}
+
+// Trial weights of bucket b's sites and their mean phi (0 for an empty
+// bucket).  Block 0 also clears the cell kernels' counters.
 __global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const double *__restrict__ d,
                              const double *__restrict__ tptr, double *__restrict__ wt,
-                             double *__restrict__ phibar)
+                             double *__restrict__ phibar, int *counters, int ncounters)
 {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    int nb = g.bx * g.by;
-    if (b >= nb) return;
-    double t = (d != nullptr && tptr != nullptr) ? *tptr : 0.0;
-    int s0 = g.bstart[b], s1 = g.bstart[b + 1];
+    if (blockIdx.x == 0 && (int)threadIdx.x < ncounters) counters[threadIdx.x] = 0;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= g.bx * g.by) return;
+    const double t = (d != nullptr && tptr != nullptr) ? *tptr : 0.0;
+    const int s0 = g.bstart[b], s1 = g.bstart[b + 1];
     double acc = 0.0;
     for (int j = s0; j < s1; j++) {
-        double wj = w[j];
-        // no contraction: the trial point is w + t*d exactly as written
-        if (d != nullptr) wj = __dadd_rn(wj, __dmul_rn(t, d[j]));
+        const double wj = trial_weight(w, d, t, j);
         wt[j] = wj;
-        double2 s = g.xy[j];
-        acc += 0.5 * (s.x * s.x + s.y * s.y - wj);
+        acc = __dadd_rn(acc, half_phi(g.xy[j], wj));
     }
     phibar[b] = (s1 > s0) ? acc / (double)(s1 - s0) : 0.0;
 }
 
-// c_b = slope of phi across the neighbouring buckets, A_b = max_j c_b.s_j - phi_j.
-__global__ void k_bucket_bound(CotGeo g, const double *__restrict__ wt, const double *__restrict__ phibar)
+// Plane bound of bucket b: c_b = slope of phi across the neighbouring buckets
+// (central difference of their means, one-sided at the grid edges), A_b =
+// max_j c_b.s_j - phi_j.
+__device__ __forceinline__ void bucket_bound(const CotGeo &g, const double *__restrict__ wt,
+                                             const double *__restrict__ phibar, int b)
 {
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    int nb = g.bx * g.by;
-    if (b >= nb) return;
-    double4 st = g.tstat[b];
+    const double4 st = g.tstat[b];
     if (st.w <= 0.0) {
         g.tdyn[b] = make_double4(0.0, 0.0, -INFINITY, 0.0);
         return;
     }
-    int u = b % g.bx, v = b / g.bx;
-    double pb = phibar[b];
+    const int u = b % g.bx, v = b / g.bx;
+    const double pb = phibar[b];
     double c[2];
     for (int ax = 0; ax < 2; ax++) {
         int bp = -1, bm = -1;
@@ -103,17 +115,17 @@ __global__ void k_bucket_bound(CotGeo g, const double *__restrict__ wt, const do
             if (v + 1 < g.by && g.tstat[b + g.bx].w > 0.0) bp = b + g.bx;
             if (v > 0 && g.tstat[b - g.bx].w > 0.0) bm = b - g.bx;
         }
-        double mb = ax == 0 ? st.x : st.y;
+        const double mb = ax == 0 ? st.x : st.y;
         double val;
         if (bp >= 0 && bm >= 0) {
-            double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
-            double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
+            const double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
+            const double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
             val = (phibar[bp] - phibar[bm]) / (mp - mm);
         } else if (bp >= 0) {
-            double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
+            const double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
             val = (phibar[bp] - pb) / (mp - mb);
         } else if (bm >= 0) {
-            double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
+            const double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
             val = (pb - phibar[bm]) / (mb - mm);
         } else {
             val = mb;
@@ -122,38 +134,35 @@ __global__ void k_bucket_bound(CotGeo g, const double *__restrict__ wt, const do
         c[ax] = val;
     }
     double A = -INFINITY;
-    int s0 = g.bstart[b], s1 = g.bstart[b + 1];
+    const int s0 = g.bstart[b], s1 = g.bstart[b + 1];
     for (int j = s0; j < s1; j++) {
-        double2 s = g.xy[j];
-        double phi = 0.5 * (s.x * s.x + s.y * s.y - wt[j]);
-        A = fmax(A, c[0] * s.x + c[1] * s.y - phi);
+        const double2 s = g.xy[j];
+        A = fmax(A, c[0] * s.x + c[1] * s.y - half_phi(s, wt[j]));
     }
     g.tdyn[b] = make_double4(c[0], c[1], A, 0.0);
 }
 
-// Level L node = union of up to 2x2 level L-1 nodes.
-__global__ void k_tree_level(CotGeo g, int L)
+// Level L node q = union of up to 2x2 level L-1 nodes.
+__device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
 {
-    int q = blockIdx.x * blockDim.x + threadIdx.x;
-    int W = g.lev_w[L], H = g.lev_h[L];
-    if (q >= W * H) return;
-    int node = g.lev_off[L] + q;
-    double4 st = g.tstat[node];
+    const int W = g.lev_w[L];
+    const int node = g.lev_off[L] + q;
+    const double4 st = g.tstat[node];
     if (st.w <= 0.0) {
         g.tdyn[node] = make_double4(0.0, 0.0, -INFINITY, 0.0);
         return;
     }
-    int u = q % W, v = q / W;
-    int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1], co = g.lev_off[L - 1];
+    const int u = q % W, v = q / W;
+    const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1], co = g.lev_off[L - 1];
     double cx = 0.0, cy = 0.0;
     int cnt = 0;
     for (int bb = 0; bb < 2; bb++)
         for (int aa = 0; aa < 2; aa++) {
-            int uu = 2 * u + aa, vv = 2 * v + bb;
+            const int uu = 2 * u + aa, vv = 2 * v + bb;
             if (uu >= cw || vv >= ch) continue;
-            int cn = co + uu + vv * cw;
+            const int cn = co + uu + vv * cw;
             if (g.tstat[cn].w <= 0.0) continue;
-            double4 dy = g.tdyn[cn];
+            const double4 dy = g.tdyn[cn];
             cx += dy.x;
             cy += dy.y;
             cnt++;
@@ -163,16 +172,43 @@ __global__ void k_tree_level(CotGeo g, int L)
     double A = -INFINITY;
     for (int bb = 0; bb < 2; bb++)
         for (int aa = 0; aa < 2; aa++) {
-            int uu = 2 * u + aa, vv = 2 * v + bb;
+            const int uu = 2 * u + aa, vv = 2 * v + bb;
             if (uu >= cw || vv >= ch) continue;
-            int cn = co + uu + vv * cw;
-            double4 cs = g.tstat[cn];
+            const int cn = co + uu + vv * cw;
+            const double4 cs = g.tstat[cn];
             if (cs.w <= 0.0) continue;
-            double4 dy = g.tdyn[cn];
-            double dx = cx - dy.x, dyy = cy - dy.y;
+            const double4 dy = g.tdyn[cn];
+            const double dx = cx - dy.x, dyy = cy - dy.y;
             A = fmax(A, dy.z + dx * cs.x + dyy * cs.y + sqrt(dx * dx + dyy * dyy) * cs.z);
         }
     g.tdyn[node] = make_double4(cx, cy, A, 0.0);
+}
+
+// Bucket plane bounds, then the last block to finish builds tree levels
+// 1..lmax (the levels a certificate walk can start from; the ones above are
+// never read) -- one launch instead of one per level.
+#define TREE_THREADS 256
+__global__ void __launch_bounds__(TREE_THREADS) k_tree_build(CotGeo g, const double *__restrict__ wt,
+                                                            const double *__restrict__ phibar, int lmax,
+                                                            unsigned int *ticket)
+{
+    __shared__ bool last;
+    const int nb = g.bx * g.by;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
+        bucket_bound(g, wt, phibar, b);
+    if (lmax < 1) return;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int L = 1; L <= lmax; L++) {
+        const int cnt = g.lev_w[L] * g.lev_h[L];
+        for (int q = threadIdx.x; q < cnt; q += blockDim.x) tree_node(g, L, q);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -1898,17 +1934,16 @@ static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int block
 void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms, CotCtx &c)
 {
     cudaStream_t s = c.s;
-    int nb = g.bx * g.by;
-    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar);
-    k_bucket_bound<<<(nb + 127) / 128, 128, 0, s>>>(g, a.wt, a.phibar);
+    const int nb = g.bx * g.by;
+    // tree levels up to the first one of at most 16 nodes: the highest level
+    // any certificate walk starts from (one round of a 16- or 32-lane segment)
+    int lmax = 0;
+    while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
+    // ovf_count[0..5]: overflow list sizes and fetch counters; [7]: the ticket
+    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 6);
+    k_tree_build<<<(nb + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(
+        g, a.wt, a.phibar, lmax, reinterpret_cast<unsigned int *>(a.ovf_count + 7));
     c.launches += 2;
-    for (int L = 1; L < g.nlev; L++) {
-        int cnt = g.lev_w[L] * g.lev_h[L];
-        k_tree_level<<<(cnt + 127) / 128, 128, 0, s>>>(g, L);
-        c.launches++;
-    }
-    // the overflow list sizes and fetch counters
-    cudaMemsetAsync(a.ovf_count, 0, 6 * sizeof(int), s);
     const int sms = num_sms > 0 ? num_sms : 148;
     const bool exact = a.cen != nullptr || a.splat != nullptr || a.solid != nullptr;
     const int lpc = (exact || cells_per_warp < 2) ? 32 : 16;

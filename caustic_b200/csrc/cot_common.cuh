@@ -125,7 +125,7 @@ struct CellsArgs {
     const double *d;       // direction (nullable)
     const double *tptr;    // device scalar step (nullable => 0)
     double *wt;            // trial weights out
-    double *phibar;        // per bucket scratch
+    double *phibar;        // per bucket mean phi (scratch)
     double *mu;            // per cell mass out
     double *fc;            // per cell objective out, without its -w_i nu_i term
     int *nv;               // per cell ring size out
@@ -166,6 +166,7 @@ void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double
                    double *partials, unsigned int *ticket, int initial, CotCtx &c);
 void launch_reject(CotSolver *S, CotCtx &c);
 void launch_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S, CotCtx &c);
+void launch_reject_cond(cudaGraphConditionalHandle hc, CotSolver *S, CotCtx &c);
 void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c);
 void configure_cells_kernels();
 void launch_fcell_full(int n, const double *fc, const double *wt, const double *nu, double *out, CotCtx &c);

@@ -42,6 +42,28 @@ __device__ __forceinline__ double wmax(double v)
     return v;
 }
 
+// Sum (or max) of stride-separated partials in block order, with the loads
+// issued ahead in groups (L2 reads: partials of other blocks are never taken
+// from a stale L1 line).
+template <bool MAX>
+__device__ __forceinline__ double sum_partials(const double *p, unsigned nblocks, size_t stride)
+{
+    double r = 0.0;
+    unsigned b = 0;
+    for (; b + 8 <= nblocks; b += 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) v[q] = __ldcg(p + (size_t)(b + q) * stride);
+#pragma unroll
+        for (int q = 0; q < 8; q++) r = MAX ? fmax(r, v[q]) : r + v[q];
+    }
+    for (; b < nblocks; b++) {
+        const double v = __ldcg(p + (size_t)b * stride);
+        r = MAX ? fmax(r, v) : r + v;
+    }
+    return r;
+}
+
 // Fixed-order block reduction of one value (sum or max).  All threads call it.
 template <bool MAX>
 __device__ double block_reduce(double v, double *sh)
@@ -159,20 +181,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_eval(int n, const double
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // one thread per value, each summing the blocks in order
+    if (threadIdx.x < 7) {
+        const int k = threadIdx.x;
+        sh[k] = (k == 2 || k == 6) ? sum_partials<true>(partials + k, gridDim.x, RED_VALS)
+                                   : sum_partials<false>(partials + k, gridDim.x, RED_VALS);
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        volatile double *p = partials;
-        double r[RED_VALS] = {0, 0, 0, 0, 0, 0, 0, 0};
-        r[2] = 0.0;
-        r[6] = 0.0;
-        for (unsigned b = 0; b < gridDim.x; b++) {
-            r[0] += p[b * RED_VALS + 0];
-            r[1] += p[b * RED_VALS + 1];
-            r[2] = fmax(r[2], p[b * RED_VALS + 2]);
-            r[3] += p[b * RED_VALS + 3];
-            r[4] += p[b * RED_VALS + 4];
-            r[5] += p[b * RED_VALS + 5];
-            r[6] = fmax(r[6], p[b * RED_VALS + 6]);
-        }
+        const double *r = sh;
         CotEvalOut o;
         o.f = r[0];
         o.gtd = r[1];
@@ -200,54 +217,72 @@ void launch_reduce(const CotGeo &g, const double *mu, const double *fc, const in
 // ---------------------------------------------------------------------------
 // iteration control (single thread)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double gram_dot(const CotSolver *S, int row, const double *delta)
-{
-    const int B = 2 * S->m + 1;
-    double r = 0.0;
-    for (int c = 0; c < B; c++)
-        if (delta[c] != 0.0) r += S->G[row * COT_BASIS + c] * delta[c];
-    return r;
-}
-
 // Two-loop recursion on the Gram matrix (ot_op.cuh:291-351): delta gives
-// d = sum_j delta_j basis_j; then the descent safeguard.
-__global__ void k_begin_iteration(CotSolver *S)
+// d = sum_j delta_j basis_j; then the descent safeguard.  One warp: the
+// (2m+1)^2 matrix is staged in shared memory and every row product is a
+// warp-wide dot product.
+__global__ void __launch_bounds__(32) k_begin_iteration(CotSolver *S)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double G[COT_BASIS * COT_BASIS];
+    __shared__ double dl[COT_BASIS];
+    const int lane = threadIdx.x;
     // only at an iteration boundary: inside a device-driven loop this kernel
     // also runs before every further trial of a line search
     if (S->done || !S->need_begin) return;
-    S->need_begin = 0;
-    S->eval_mark = S->evals;
-    const int m = S->m, gi = 2 * m;
-    S->gnorm_stale = sqrt(S->gnorm2);
-    S->empty_stale = S->empty;
-    double *dl = S->delta;
-    for (int c = 0; c < COT_BASIS; c++) dl[c] = 0.0;
-    dl[gi] = -1.0;
-    int cnt = S->k < m ? S->k : m;
-    bool skip = (S->mode == COT_SOLVE_REFERENCE) && S->restart;
+    const int m = S->m, B = 2 * m + 1, gi = 2 * m;
+    for (int q = lane; q < B * B; q += 32) G[q] = S->G[(q / B) * COT_BASIS + q % B];
+    for (int c = lane; c < B; c += 32) dl[c] = (c == gi) ? -1.0 : 0.0;
+    __syncwarp();
+    auto gdot = [&](int row) -> double {
+        double r = 0.0;
+        for (int c = lane; c < B; c += 32) r += G[row * B + c] * dl[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(FULLMASK, r, o);
+        return r;
+    };
+    const int cnt = S->k < m ? S->k : m;
+    const bool skip = (S->mode == COT_SOLVE_REFERENCE) && S->restart;
+    double alpha[COT_MAX_HIST];
     if (!skip) {
         for (int i = 1; i <= cnt; i++) {
-            int idx = ((S->k - i) % m + m) % m;
-            S->alpha[idx] = gram_dot(S, idx, dl) * S->rho[idx];
-            dl[m + idx] -= S->alpha[idx];
+            const int idx = ((S->k - i) % m + m) % m;
+            const double a = gdot(idx) * S->rho[idx];
+            alpha[i - 1] = a;
+            __syncwarp();
+            if (lane == 0) dl[m + idx] -= a;
+            __syncwarp();
         }
-        for (int c = 0; c < COT_BASIS; c++) dl[c] *= S->H0;
+        const double H0 = S->H0;
+        for (int c = lane; c < B; c += 32) dl[c] *= H0;
+        __syncwarp();
         for (int i = cnt; i > 0; i--) {
-            int idx = ((S->k - i) % m + m) % m;
-            double beta = S->rho[idx] * gram_dot(S, m + idx, dl);
-            dl[idx] += S->alpha[idx] - beta;
+            const int idx = ((S->k - i) % m + m) % m;
+            const double beta = S->rho[idx] * gdot(m + idx);
+            __syncwarp();
+            if (lane == 0) dl[idx] += alpha[i - 1] - beta;
+            __syncwarp();
         }
     }
-    double gd = gram_dot(S, gi, dl);
-    if (!(gd < 0.0)) {
-        for (int c = 0; c < COT_BASIS; c++) dl[c] = 0.0;
-        dl[gi] = -1.0;
+    double gd = gdot(gi);
+    __syncwarp();
+    const bool reset = !(gd < 0.0);  // not a descent direction: steepest descent
+    if (reset) {
+        for (int c = lane; c < B; c += 32) dl[c] = (c == gi) ? -1.0 : 0.0;
+        gd = -G[gi * B + gi];
+    }
+    __syncwarp();
+    for (int c = lane; c < COT_BASIS; c += 32) S->delta[c] = c < B ? dl[c] : 0.0;
+    if (lane != 0) return;
+    if (!skip)
+        for (int i = 1; i <= cnt; i++) S->alpha[((S->k - i) % m + m) % m] = alpha[i - 1];
+    if (reset) {
         S->k = 0;
         S->H0 = 1.0;
-        gd = -S->G[gi * COT_BASIS + gi];
     }
+    S->need_begin = 0;
+    S->eval_mark = S->evals;
+    S->gnorm_stale = sqrt(S->gnorm2);
+    S->empty_stale = S->empty;
     S->gd = gd;
     S->t = S->t0;
     S->lo = 0.0;
@@ -384,12 +419,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
     __syncthreads();
     if (!last) return;
     __threadfence();
-    volatile double *p = partials;
-    for (int v = threadIdx.x; v < nvals; v += blockDim.x) {
-        double r = 0.0;
-        for (unsigned b = 0; b < gridDim.x; b++) r += p[(size_t)b * nvals + v];
-        tot[v] = r;
-    }
+    for (int v = threadIdx.x; v < nvals; v += blockDim.x) tot[v] = sum_partials<false>(partials + v, gridDim.x, nvals);
     __syncthreads();
     if (threadIdx.x != 0) return;
     *ticket = 0u;
@@ -446,7 +476,7 @@ void launch_accept(const CotGeo &g, CotSolver *S, double *Sv, double *Yv, double
 }
 
 // Line search gave up (ot_op.cuh:413-425): keep the point, drop the history.
-__global__ void k_reject(CotSolver *S)
+__device__ __forceinline__ void reject(CotSolver *S)
 {
     if (S->done || S->accepted || S->ls_active) return;
     S->need_begin = 1;
@@ -463,6 +493,8 @@ __global__ void k_reject(CotSolver *S)
     S->iter++;
     if (S->iter >= S->max_iter) S->done = 1;
 }
+
+__global__ void k_reject(CotSolver *S) { reject(S); }
 
 void launch_reject(CotSolver *S, CotCtx &c)
 {
@@ -481,6 +513,20 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S)
 void launch_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S, CotCtx &c)
 {
     k_loop_cond<<<1, 1, 0, c.s>>>(hc, S);
+    c.launches++;
+}
+
+// The end of a pass of the device-driven trial loop: reject (if the line
+// search just gave up) and the loop condition, in one launch.
+__global__ void k_reject_cond(cudaGraphConditionalHandle hc, CotSolver *S)
+{
+    reject(S);
+    cudaGraphSetConditional(hc, (!S->done && S->iter < S->pause_iter) ? 1u : 0u);
+}
+
+void launch_reject_cond(cudaGraphConditionalHandle hc, CotSolver *S, CotCtx &c)
+{
+    k_reject_cond<<<1, 1, 0, c.s>>>(hc, S);
     c.launches++;
 }
 
