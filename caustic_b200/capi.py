@@ -41,7 +41,7 @@ EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
     "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_source_masses_point_light", "cot_last_error",
-    "cot_set_progress",
+    "cot_set_progress", "cot_solve_batch",
 ]
 # int (*)(void *user, int phase, int iteration, int status, const double *w, const double *nu, int n,
 #         double grad_norm, double max_rel_err)
@@ -120,6 +120,8 @@ def load():
                                      ctypes.POINTER(cot_solve_stats)]
         L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.cot_set_progress.argtypes = [vp, PROGRESS_FN, vp, ctypes.c_int]
+        L.cot_solve_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp),
+                                      ctypes.POINTER(cot_solve_opts), ctypes.POINTER(cot_solve_stats)]
         for name in EXPORTED:
             getattr(L, name).restype = ctypes.c_int
         _lib = L
@@ -385,3 +387,28 @@ def _tptr(t):
     if not t.is_cuda or t.dtype not in (torch.float64, torch.uint8) or not t.is_contiguous():
         raise ValueError("device arrays must be contiguous CUDA tensors (float64)")
     return ctypes.c_void_p(t.data_ptr())
+
+
+def solve_batch(solvers, w0s, mode=SOLVE_WOLFE, history=10, max_iter=20000, tol=1e-4, initial_step=1.0, c1=0.0,
+                c2=0.0, max_ls=0, raise_on_noconv=False):
+    """Solve one problem per solver (all on one device) in a single graph
+    launch on the first solver's stream (cot_solve_batch).  w0s: host start
+    weights, one array per solver.  Returns (weights, stats), one entry per
+    solver; every stats' ms is the time of the whole batch."""
+    L = load()
+    n = len(solvers)
+    if n == 0 or len(w0s) != n:
+        raise ValueError("one start vector per solver")
+    ws = [_f64(w).copy() for w in w0s]
+    for s_, w in zip(solvers, ws):
+        if w.size != s_.n:
+            raise ValueError("start vector of the wrong size")
+    hs = (ctypes.c_void_p * n)(*[s_._h.value for s_ in solvers])
+    wp = (ctypes.c_void_p * n)(*[w.ctypes.data for w in ws])
+    opts = cot_solve_opts(mode, history, max_iter, tol, initial_step, c1, c2, max_ls, 0)
+    st = (cot_solve_stats * n)()
+    rc = L.cot_solve_batch(hs, n, wp, ctypes.byref(opts), st)
+    solvers[0]._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV,))
+    stats = [SolveStats(x.iterations, x.evaluations, x.restarts, bool(x.converged), x.f, x.max_rel_err, x.grad_norm,
+                        x.empty_cells, x.ring_overflows, x.ms) for x in st]
+    return ws, stats

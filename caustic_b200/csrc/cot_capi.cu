@@ -836,6 +836,35 @@ static int report_progress(cot_handle *h, int phase, int iteration, int status, 
     return COT_OK;
 }
 
+// One pass of the device-driven trial loop (the body of its WHILE node).
+static void launch_trial_body(cot_handle *h, cudaGraphConditionalHandle hc, double *tptr, CotCtx &c)
+{
+    CotProblemDev &P = h->P;
+    launch_begin_iteration(P.S, c);
+    launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, c);
+    CellsArgs a = cells_args(P, P.w, P.d, tptr);
+    launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, c);
+    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, c);
+    launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, c);
+    launch_reject_cond(hc, P.S, c);
+}
+
+// The first point of a solve: its evaluation becomes the current point.
+static void launch_first_point(cot_handle *h, CotCtx &c)
+{
+    CotProblemDev &P = h->P;
+    CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
+    launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, c);
+    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, c);
+    launch_init_from_eval(P.S, P.out, c);
+    launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, c);
+}
+
+static double *step_ptr(CotProblemDev &P)
+{
+    return reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
+}
+
 // Counters that one body of the trial graph adds per execution.
 struct BodyCounts {
     long long launches = 0, cell_launches = 0, evaluations = 0;
@@ -851,7 +880,6 @@ struct BodyCounts {
 // host-driven loop).
 static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec, BodyCounts *bc)
 {
-    CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
     *exec = nullptr;
     if (s == nullptr || s == cudaStreamLegacy) return COT_EINVAL;  // the legacy stream cannot be captured
@@ -879,13 +907,7 @@ static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec,
     CotCtx &c = h->c();
     const CotCtx saved = c;
     c.profile = false;
-    launch_begin_iteration(P.S, c);
-    launch_direction(P.geo, P.S, P.Sv, P.Yv, P.mu, P.d, c);
-    CellsArgs a = cells_args(P, P.w, P.d, tptr);
-    launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, c);
-    launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, P.d, h->cfg.max_ring, P.partials, P.ticket, P.out, P.S, c);
-    launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 0, c);
-    launch_reject_cond(hc, P.S, c);
+    launch_trial_body(h, hc, tptr, c);
     cudaGraph_t captured = nullptr;
     e = cudaStreamEndCapture(s, &captured);
     bc->launches = c.launches - saved.launches;
@@ -902,8 +924,9 @@ static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec,
     return COT_OK;
 }
 
-static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms, int phase,
-                        bool report_start)
+// History buffers and the device control block of a solve from the weights
+// in P.w, on the handle's stream.
+static int solve_prepare(cot_handle *h, const cot_solve_opts &o)
 {
     CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
@@ -938,18 +961,22 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
     hs.pause_iter = INT_MAX;
     if (o.max_iter == 0) hs.done = 1;
     COT_CUDA_TRY(cudaMemcpyAsync(P.S, &hs, sizeof(CotSolver), cudaMemcpyHostToDevice, s));
+    return COT_OK;
+}
+
+static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms, int phase,
+                        bool report_start)
+{
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    CotSolver &hs = *h->hS;
+    int rp;
+    if ((rp = solve_prepare(h, o)) != COT_OK) return rp;
     cudaEvent_t e0, e1;
     COT_CUDA_TRY(cudaEventCreate(&e0));
     COT_CUDA_TRY(cudaEventCreate(&e1));
     COT_CUDA_TRY(cudaEventRecord(e0, s));
-    // first point
-    {
-        CellsArgs a = cells_args(P, P.w, nullptr, nullptr);
-        launch_eval(P.geo, a, h->cfg.cells_per_warp, h->num_sms, h->c());
-        launch_reduce(P.geo, P.mut, P.fc, P.nv, P.wt, nullptr, h->cfg.max_ring, P.partials, P.ticket, P.out, nullptr, h->c());
-        launch_init_from_eval(P.S, P.out, h->c());
-        launch_accept(P.geo, P.S, P.Sv, P.Yv, P.w, P.wt, P.mu, P.mut, P.d, P.partials, P.ticket, 1, h->c());
-    }
+    launch_first_point(h, h->c());
     if (h->prog_fn && report_start) {
         // the starting point (iteration -1)
         COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s));
@@ -967,7 +994,7 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
     }
     const size_t ctl = 16 * sizeof(int);
     int reported = 0;
-    double *tptr = reinterpret_cast<double *>(reinterpret_cast<char *>(P.S) + offsetof(CotSolver, t));
+    double *tptr = step_ptr(P);
     // progress report at an iteration boundary (hs holds the control block)
     auto boundary_report = [&]() -> int {
         if (!(h->prog_fn && hs.iter > 0 && hs.iter != reported && ((hs.iter - 1) % h->prog_every == 0 || hs.done)))
@@ -1102,6 +1129,137 @@ extern "C" int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *o
     COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
     fill_stats(hs, ms, stats);
     if (!hs.converged) return failf(h, COT_ENOTCONV, "cot_solve: stopped after %d iterations (max rel err %.3e)", hs.iter, hs.maxrel);
+    return COT_OK;
+}
+
+// Many independent solves in one graph launch: handle k's solve is one
+// branch (its first evaluation, then its own WHILE node over the trial
+// body), so the branches run concurrently and small instances overlap.
+extern "C" int cot_solve_batch(cot_handle *const *hs_in, int count, double *const *w_inout,
+                               const cot_solve_opts *opts, cot_solve_stats *stats)
+{
+    if (!hs_in || count <= 0 || !hs_in[0]) return COT_EINVAL;
+    cot_handle *h0 = hs_in[0];
+    if (!w_inout || !opts) return fail(h0, COT_EINVAL, "cot_solve_batch: NULL argument", nullptr);
+    for (int k = 0; k < count; k++) {
+        cot_handle *h = hs_in[k];
+        if (!h || !w_inout[k]) return failf(h0, COT_EINVAL, "cot_solve_batch: entry %d is NULL", k);
+        if (!h->has_problem) return failf(h0, COT_ENOPROBLEM, "cot_solve_batch: handle %d has no problem", k);
+        if (h->device != h0->device) return failf(h0, COT_EINVAL, "cot_solve_batch: handle %d is on another device", k);
+        for (int j = 0; j < k; j++)
+            if (hs_in[j] == h) return failf(h0, COT_EINVAL, "cot_solve_batch: handle %d appears twice", k);
+    }
+    cot_solve_opts o = *opts;
+    int r;
+    if ((r = check_opts(h0, o)) != COT_OK) return r;
+    {
+        const cudaError_t ed = cudaSetDevice(h0->device);
+        if (ed != cudaSuccess) return fail(h0, COT_ECUDA, "cot_solve_batch: cudaSetDevice", cudaGetErrorString(ed));
+    }
+    cudaStream_t s = h0->stream;
+    if (s == nullptr || s == cudaStreamLegacy)
+        return fail(h0, COT_EINVAL, "cot_solve_batch: the first handle's stream cannot be captured (legacy default stream)",
+                    nullptr);
+    // every handle works on the batch stream for the set-up and the capture
+    std::vector<cudaStream_t> saved(count);
+    for (int k = 0; k < count; k++) {
+        saved[k] = hs_in[k]->stream;
+        hs_in[k]->stream = s;
+    }
+    auto restore = [&]() {
+        for (int k = 0; k < count; k++) hs_in[k]->stream = saved[k];
+    };
+    auto bail = [&](int code) {
+        restore();
+        return code;
+    };
+    for (int k = 0; k < count; k++) {
+        if ((r = upload_sorted(hs_in[k], w_inout[k], COT_MEM_HOST, hs_in[k]->P.w)) != COT_OK) return bail(r);
+        if ((r = solve_prepare(hs_in[k], o)) != COT_OK) return bail(r);
+    }
+    cudaGraph_t G = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<BodyCounts> first(count), body(count);
+    cudaError_t e = cudaGraphCreate(&G, 0);
+    for (int k = 0; k < count && e == cudaSuccess; k++) {
+        cot_handle *h = hs_in[k];
+        CotCtx &c = h->c();
+        const CotCtx keep = c;
+        c.profile = false;
+        cudaGraph_t child = nullptr;
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            launch_first_point(h, c);
+            e = cudaStreamEndCapture(s, &child);
+        }
+        first[k].launches = c.launches - keep.launches;
+        first[k].cell_launches = c.cell_launches - keep.cell_launches;
+        first[k].evaluations = c.evaluations - keep.evaluations;
+        cudaGraphNode_t n1 = nullptr, cn = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n1, G, nullptr, 0, child);
+        if (child) cudaGraphDestroy(child);
+        cudaGraphConditionalHandle hc;
+        cudaGraphNodeParams cp = {};
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hc, G, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = hc;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            e = cudaGraphAddNode(&cn, G, &n1, 1, &cp);
+        }
+        if (e == cudaSuccess)
+            e = cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+        const long long l0 = c.launches, cl0 = c.cell_launches, ev0 = c.evaluations;
+        if (e == cudaSuccess) {
+            launch_trial_body(h, hc, step_ptr(h->P), c);
+            cudaGraph_t captured = nullptr;
+            e = cudaStreamEndCapture(s, &captured);
+        }
+        body[k].launches = c.launches - l0;
+        body[k].cell_launches = c.cell_launches - cl0;
+        body[k].evaluations = c.evaluations - ev0;
+        c = keep;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, G, 0);
+    if (G) cudaGraphDestroy(G);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail(h0, COT_ECUDA, "cot_solve_batch: graph", cudaGetErrorString(e)));
+    }
+    cudaEvent_t e0, e1;
+    e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(exec);
+    if (e != cudaSuccess) return bail(fail(h0, COT_ECUDA, "cot_solve_batch: launch", cudaGetErrorString(e)));
+    int unconverged = 0;
+    for (int k = 0; k < count; k++) {
+        cot_handle *h = hs_in[k];
+        CotSolver &hs = *h->hS;
+        e = cudaMemcpyAsync(h->hS, h->P.S, sizeof(CotSolver), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && (r = download_sorted(h, h->P.w, w_inout[k], COT_MEM_HOST)) != COT_OK) return bail(r);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return bail(fail(h0, COT_ECUDA, "cot_solve_batch: results", cudaGetErrorString(e)));
+        const long long bodies = hs.evals > 0 ? hs.evals - 1 : 0;
+        h->ctx.launches += first[k].launches + bodies * body[k].launches;
+        h->ctx.cell_launches += first[k].cell_launches + bodies * body[k].cell_launches;
+        h->ctx.evaluations += first[k].evaluations + bodies * body[k].evaluations;
+        if (stats) fill_stats(hs, ms, &stats[k]);
+        if (!hs.converged) unconverged++;
+    }
+    restore();
+    if (unconverged)
+        return failf(h0, COT_ENOTCONV, "cot_solve_batch: %d of %d solves stopped before the tolerance", unconverged,
+                     count);
     return COT_OK;
 }
 

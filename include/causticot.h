@@ -164,6 +164,20 @@ COT_API int cot_cells(cot_handle *h, const double *w, int *ring_offsets, double 
 COT_API int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts,
               cot_solve_stats *stats, int mem);
 
+/* Solve count independent problems, one per handle (all on one device,
+ * each handle at most once), in a single CUDA graph launch on the first
+ * handle's stream (which must not be the legacy default stream): handle k's
+ * solve is one branch of the graph -- its first evaluation, then its own
+ * device-driven trial loop -- and the branches run concurrently, so many
+ * small instances share the GPU instead of queueing.  w_inout[k]: host array
+ * of handle k's n weights (start in, result out).  stats (nullable): count
+ * entries; their ms is the time of the whole batch.  Progress callbacks are
+ * not called.  COT_ENOTCONV when some solve stopped before the tolerance
+ * (its stats say which).  Errors are reported on the first handle.  Replaces
+ * running the reference's caustic_GPU once per instance. */
+COT_API int cot_solve_batch(cot_handle *const *handles, int count, double *const *w_inout,
+                            const cot_solve_opts *opts, cot_solve_stats *stats);
+
 /* Inputs of the Fresnel-reweighted solve (host arrays, caller order). */
 typedef struct {
     const double *points_xy;     /* source (lens) sites, 2n */
