@@ -2,7 +2,10 @@
 
 ``libcausticot.so`` (the C ABI in include/causticot.h) is compiled in-tree
 for sm_100a with nvcc; ``caustic_GPU`` (the process + file shim of the
-reference executable) links against it.
+reference executable) links against it.  ``libcausticws.so`` (the warm-start
+network's kernels, include/causticws.h) is built apart because its
+tensor-core GEMMs come from the CUTLASS sm100 templates, which take a while
+to compile.
 """
 from __future__ import annotations
 
@@ -17,6 +20,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libcausticot.so")
 CLI = os.path.join(PKG, "caustic_GPU")
 CU_SOURCES = ["cot_cells.cu", "cot_solver.cu", "cot_capi.cu", "cot_noalloc.cu"]
+WS_LIB = os.path.join(PKG, "libcausticws.so")
+WS_SOURCES = ["wsn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -59,9 +64,47 @@ def build_cli(force: bool = False) -> str:
     return CLI
 
 
+def cutlass_dirs() -> list:
+    """Include directories of a CUTLASS tree with the sm100 collectives
+    (CUTLASS_DIR, else the copies vendored by installed packages)."""
+    cands = []
+    if os.environ.get("CUTLASS_DIR"):
+        cands.append(os.environ["CUTLASS_DIR"])
+    try:
+        import site
+
+        for sp in site.getsitepackages():
+            cands.append(os.path.join(sp, "flashinfer", "data", "cutlass"))
+            cands.append(os.path.join(sp, "tilelang", "3rdparty", "cutlass"))
+    except Exception:
+        pass
+    for c in cands:
+        inc = os.path.join(c, "include")
+        if os.path.exists(os.path.join(inc, "cutlass", "gemm", "collective", "builders", "sm100_umma_builder.inl")):
+            return [inc, os.path.join(c, "tools", "util", "include")]
+    raise RuntimeError("no CUTLASS tree with the sm100 collectives found (set CUTLASS_DIR)")
+
+
+def build_ws(force: bool = False, verbose: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in WS_SOURCES]
+    deps = srcs + [os.path.join(ROOT, "include", "causticws.h")]
+    if not force and not _stale(WS_LIB, deps):
+        return WS_LIB
+    inc = []
+    for d in cutlass_dirs():
+        inc += ["-I", d]
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-diag-suppress", "20012",
+           *inc, "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-o", WS_LIB, *srcs]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    return WS_LIB
+
+
 def build(force: bool = False, verbose: bool = False):
     build_lib(force, verbose)
     build_cli(force)
+    build_ws(force, verbose)
 
 
 if __name__ == "__main__":
