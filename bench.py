@@ -407,12 +407,65 @@ def run_batch(args):
     return 0
 
 
+def run_warmstart(args):
+    """The learned warm start: the network trained on 2,000 solver-made
+    pairs (caustic_b200/data/warmstart_c4.npz, made by
+    `python -m caustic_b200.warmstart`) starts the solves of held-out seeds
+    of the configuration (128^2 jittered sites, 256^2 targets, K in 2..16);
+    the same solves from w = 0 run beside them.  Both arms run to max-rel
+    1e-4 as batched solves of 64; a step is one chunk of 64 instances."""
+    import numpy as np
+    import torch
+
+    from caustic_b200 import problems, warmstart
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    path = os.path.join(ROOT, "caustic_b200", "data", "warmstart_c4.npz")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "ours", "unavailable": f"no trained network at {os.path.relpath(path, ROOT)}"}))
+        return 0
+    net = warmstart.WarmStartNet.from_file(path)
+    warm = [problems.make(4, 200000 + i) for i in range(8)]
+    for _ in range(args.warmup):
+        warmstart.compare(net, warm, tol=args.tol, history=args.history)
+    probs = [problems.make(4, 100000 + i) for i in range(64 * args.steps)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    res = {}
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            torch.cuda.synchronize()
+            r = warmstart.compare(net, probs[64 * k:64 * (k + 1)], tol=args.tol, history=args.history)
+            for key, v in r.items():
+                res[key] = res.get(key, 0.0 if not isinstance(v, list) else []) + v
+    n = len(probs)
+    line = {"metric": "OT solve ms @1e-4 mass err: learned warm-start vs plain L-BFGS", "impl": "ours",
+            "value": 1e3 * res["warm_s"] / n, "unit": "ms/solve", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 solve, bf16 network", "data": "synthetic (seeded held-out instances of the warm-start configuration)",
+            "config": {"workload": "sdot_config4_warmstart", "n_sites": probs[0].n, "image": list(probs[0].size),
+                       "held_out": n, "train_pairs": 2000, "stop": "max_rel_mass_err<=1e-4",
+                       "batched": 64, "l2": "256 MiB buffer written between chunks"},
+            "cold_ms_per_solve": 1e3 * res["cold_s"] / n, "warm_ms_per_solve": 1e3 * res["warm_s"] / n,
+            "inference_ms_per_solve": 1e3 * res["infer_s"] / n,
+            "speedup": res["cold_s"] / res["warm_s"],
+            "cold_iterations_mean": float(np.mean(res["cold_iters"])),
+            "warm_iterations_mean": float(np.mean(res["warm_iters"])),
+            "cold_max_rel_err": float(max(res["cold_err"])), "warm_max_rel_err": float(max(res["warm_err"])),
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == 3:
         return run_batch(args)
+    if args.config == 4:
+        return run_warmstart(args)
     return run_ours(args)
 
 

@@ -244,13 +244,17 @@ __global__ void k_take_channels(long long P, int Cn, const float *__restrict__ d
     }
 }
 
-// Mean-free squared error per sample: the weights are defined up to a
-// constant, so prediction and target are compared after removing each one's
-// mean.  loss = sum_b mean_i (e_bi - mean_i e_bi)^2 / B, grad d loss / d p.
-__global__ void k_mse_centered(int B, int n, const float *__restrict__ p, const float *__restrict__ t,
-                               float *__restrict__ grad, float *__restrict__ loss_b)
+// Mean-free error per sample on a gy x gx grid: the weights are defined up
+// to a constant, so prediction and target are compared after removing each
+// one's mean.  With e = pred - target - mean:
+//   loss_b = [ sum_i e_i^2 + lambda * sum (forward differences of e)^2 ] / (n B)
+// (the second term weighs the local differences that set the cells' masses)
+// and grad = d(sum_b loss_b) / d pred.
+__global__ void k_mse_centered(int B, int gy, int gx, float lambda, const float *__restrict__ p,
+                               const float *__restrict__ t, float *__restrict__ grad, float *__restrict__ loss_b)
 {
     __shared__ float sh[T];
+    const int n = gy * gx;
     const int b = blockIdx.x;
     const float *pb = p + (long long)b * n;
     const float *tb = t + (long long)b * n;
@@ -264,11 +268,30 @@ __global__ void k_mse_centered(int B, int n, const float *__restrict__ p, const 
     }
     const float mean = sh[0] / n;
     __syncthreads();
+    const float sc = 1.f / ((float)n * B);
     float l = 0.f;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int x = i % gx, y = i / gx;
         const float e = pb[i] - tb[i] - mean;
+        float g = 2.f * e;
         l += e * e;
-        grad[(long long)b * n + i] = 2.f * e / ((float)n * B);
+        if (lambda != 0.f) {
+            // differences to the right / upper neighbour (counted once) and
+            // the gradient of every difference this site is part of
+            if (x + 1 < gx) {
+                const float d = (pb[i + 1] - tb[i + 1] - mean) - e;
+                l += lambda * d * d;
+                g -= 2.f * lambda * d;
+            }
+            if (x > 0) g += 2.f * lambda * (e - (pb[i - 1] - tb[i - 1] - mean));
+            if (y + 1 < gy) {
+                const float d = (pb[i + gx] - tb[i + gx] - mean) - e;
+                l += lambda * d * d;
+                g -= 2.f * lambda * d;
+            }
+            if (y > 0) g += 2.f * lambda * (e - (pb[i - gx] - tb[i - gx] - mean));
+        }
+        grad[(long long)b * n + i] = g * sc;
     }
     sh[threadIdx.x] = l;
     __syncthreads();
@@ -276,7 +299,7 @@ __global__ void k_mse_centered(int B, int n, const float *__restrict__ p, const 
         if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) loss_b[b] = sh[0] / ((float)n * B);
+    if (threadIdx.x == 0) loss_b[b] = sh[0] * sc;
 }
 
 // Adam on fp32 master weights, with the bf16 copy the GEMMs read
@@ -429,10 +452,11 @@ WS_API int ws_take_channels(long long P, int C, const float *dout, int Ct, int c
     return last_error();
 }
 
-WS_API int ws_mse_centered(int B, int n, const float *pred, const float *target, float *grad, float *loss_b,
-                           void *stream)
+WS_API int ws_mse_centered(int B, int gy, int gx, float lambda, const float *pred, const float *target, float *grad,
+                           float *loss_b, void *stream)
 {
-    k_mse_centered<<<B, T, 0, static_cast<cudaStream_t>(stream)>>>(B, n, pred, target, grad, loss_b);
+    if (B <= 0 || gy <= 0 || gx <= 0) return WS_EINVAL;
+    k_mse_centered<<<B, T, 0, static_cast<cudaStream_t>(stream)>>>(B, gy, gx, lambda, pred, target, grad, loss_b);
     return last_error();
 }
 

@@ -60,7 +60,7 @@ def load():
         L.ws_up2_back.argtypes = [i, i, i, i, vp, i, i, vp, vp]
         L.ws_put_channels.argtypes = [ll, i, vp, i, i, vp, vp]
         L.ws_take_channels.argtypes = [ll, i, vp, i, i, i, vp, vp]
-        L.ws_mse_centered.argtypes = [i, i, vp, vp, vp, vp, vp]
+        L.ws_mse_centered.argtypes = [i, i, i, f, vp, vp, vp, vp, vp]
         L.ws_adam.argtypes = [ll, vp, vp, vp, vp, vp, f, f, f, f, i, vp]
         L.ws_to_bf16.argtypes = [ll, vp, vp, vp]
         for name in ("ws_gemm", "ws_im2col", "ws_col2im", "ws_bias_act", "ws_act_back", "ws_colsum", "ws_pool2",
@@ -326,14 +326,20 @@ class WarmStartNet:
                 _ok(L.ws_adam(c.b.numel(), _p(c.b), None, _p(c.gb), _p(c.state[2]), _p(c.state[3]), lr, b1, b2, eps,
                               self.step, self._stream), "adam")
 
-    def loss_grad(self, pred, target):
-        """Mean-free squared error (ws_mse_centered): (loss, dpred)."""
+    def loss_grad(self, pred, target, grid=None, lam: float = 0.0):
+        """Mean-free squared error on the site grid (ws_mse_centered), with
+        lam weighing the neighbour differences: (loss, dpred).  grid =
+        (gy, gx), default square."""
         torch = self.torch
         L = load()
         Bn, n = pred.shape
+        gy, gx = grid if grid else (int(round(np.sqrt(n))),) * 2
+        if gy * gx != n:
+            raise ValueError("grid does not match the prediction")
         grad = torch.empty_like(pred)
         lb = torch.empty(Bn, dtype=torch.float32, device=self.dev)
-        _ok(L.ws_mse_centered(Bn, n, _p(pred), _p(target.contiguous()), _p(grad), _p(lb), self._stream), "mse")
+        _ok(L.ws_mse_centered(Bn, gy, gx, float(lam), _p(pred), _p(target.contiguous()), _p(grad), _p(lb),
+                              self._stream), "mse")
         return float(lb.sum()), grad
 
 
@@ -415,7 +421,7 @@ def solve_pairs(probs, tol: float = 1e-5, history: int = 10, chunk: int = 64):
 
 
 def fit(net: WarmStartNet, X, Y, *, epochs: int = 30, batch: int = 16, lr: float = 1e-3, seed: int = 0,
-        log=None) -> list:
+        lam: float = 0.0, log=None) -> list:
     """Adam on the mean-free squared error.  X: bf16 [S, H, W, 8], Y: fp32
     [S, H*W] (device).  Returns the mean loss of every epoch."""
     torch = net.torch
@@ -429,7 +435,7 @@ def fit(net: WarmStartNet, X, Y, *, epochs: int = 30, batch: int = 16, lr: float
             idx = order[k:k + batch]
             net.zero_grad()
             pred = net.forward(X.index_select(0, idx), keep=True)
-            loss, g = net.loss_grad(pred, Y.index_select(0, idx))
+            loss, g = net.loss_grad(pred, Y.index_select(0, idx), grid=tuple(X.shape[1:3]), lam=lam)
             net.backward(g)
             net.adam(lr=lr)
             tot += loss
@@ -498,6 +504,7 @@ def main(argv=None) -> int:
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lam", type=float, default=0.0, help="weight of the neighbour-difference term of the loss")
     ap.add_argument("--levels", type=int, default=4)
     ap.add_argument("--base", type=int, default=32)
     ap.add_argument("--grid", type=int, default=0, help="sites per side (0: the configuration's 128)")
@@ -519,13 +526,13 @@ def main(argv=None) -> int:
     Y, net.out_scale = make_target(ws)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    hist = fit(net, X, Y, epochs=a.epochs, batch=a.batch, lr=a.lr)
+    hist = fit(net, X, Y, epochs=a.epochs, batch=a.batch, lr=a.lr, lam=a.lam)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
     if a.out:
         np.savez(a.out, **net.state_dict())
     res = compare(net, held, tol=1e-4)
-    line = {"pairs": a.pairs, "held": a.held, "n_sites": train[0].n, "image": list(train[0].size),
+    line = {"pairs": a.pairs, "held": a.held, "n_sites": train[0].n, "image": list(train[0].size), "lam": a.lam,
             "data_s": t_data, "pairs_converged": int(sum(s.converged for s in st)),
             "train_s": t_train, "epochs": a.epochs, "loss_first": hist[0], "loss_last": hist[-1],
             "cold_iters_mean": float(np.mean(res["cold_iters"])), "warm_iters_mean": float(np.mean(res["warm_iters"])),

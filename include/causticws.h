@@ -72,12 +72,14 @@ WS_API int ws_put_channels(long long P, int C, const void *in, int Ct, int c0, v
 WS_API int ws_take_channels(long long P, int C, const float *dout, int Ct, int c0, int add, float *din,
                             void *stream);
 
-/* Loss of B predictions of n weights against their targets, each compared
- * after removing its mean (weights are defined up to a constant):
- * loss_b[b] = mean_i (e_bi - mean e_b)^2 / B with e = pred - target, and
- * grad = d(sum_b loss_b) / d pred. */
-WS_API int ws_mse_centered(int B, int n, const float *pred, const float *target, float *grad, float *loss_b,
-                           void *stream);
+/* Loss of B predictions of the weights of a gy x gx site grid (row-major)
+ * against their targets, each compared after removing its mean (weights are
+ * defined up to a constant).  With e = pred - target minus its mean:
+ * loss_b[b] = (sum e^2 + lambda * sum of the squared differences of e between
+ * grid neighbours) / (gy gx B); grad = d(sum_b loss_b) / d pred.  The
+ * difference term weighs the local structure that sets the cells' masses. */
+WS_API int ws_mse_centered(int B, int gy, int gx, float lambda, const float *pred, const float *target,
+                           float *grad, float *loss_b, void *stream);
 
 /* Adam step `step` (1-based) on fp32 weights w, refreshing their bf16 copy
  * w16 (nullable). */

@@ -145,8 +145,20 @@ class Net:
         return grads
 
 
-def loss_grad(pred, target):
+def loss_grad(pred, target, grid=None, lam=0.0):
+    """Mean-free squared error with lam weighing the squared differences
+    between grid neighbours (grid = (gy, gx), row-major; default square)."""
     B, n = pred.shape
+    gy, gx = grid if grid else (int(round(np.sqrt(n))),) * 2
     e = pred - target
     e = e - e.mean(axis=1, keepdims=True)
-    return float((e * e).sum() / (n * B)), 2.0 * e / (n * B)
+    E = e.reshape(B, gy, gx)
+    dx = E[:, :, 1:] - E[:, :, :-1]
+    dy = E[:, 1:, :] - E[:, :-1, :]
+    loss = ((e * e).sum() + lam * ((dx * dx).sum() + (dy * dy).sum())) / (n * B)
+    G = 2.0 * E
+    G[:, :, 1:] += 2.0 * lam * dx
+    G[:, :, :-1] -= 2.0 * lam * dx
+    G[:, 1:, :] += 2.0 * lam * dy
+    G[:, :-1, :] -= 2.0 * lam * dy
+    return float(loss), G.reshape(B, n) / (n * B)

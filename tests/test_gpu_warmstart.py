@@ -48,14 +48,14 @@ def test_network_matches_oracle(gpu):
     x = R.bf16(rng.normal(size=(2, 16, 16, warmstart.IN_CH)))
     t = rng.normal(size=(2, 256))
     pred = net.forward(bf16_tensor(torch, x), keep=True)
-    loss, g = net.loss_grad(pred, torch.from_numpy(t.astype(np.float32)).cuda())
+    loss, g = net.loss_grad(pred, torch.from_numpy(t.astype(np.float32)).cuda(), lam=5.0)
     net.zero_grad()
     net.backward(g)
     ref = R.Net([(c.w.cpu().numpy().astype(np.float64),
                   None if c.b is None else c.b.cpu().numpy().astype(np.float64)) for c in net.layers()],
                 net.levels, net.ch)
     rp = ref.forward(x)
-    rl, rg = R.loss_grad(rp, t)
+    rl, rg = R.loss_grad(rp, t, lam=5.0)
     grads = ref.backward(rg)
     p = pred.cpu().numpy()
     assert np.abs(p - rp).max() <= 2e-2 * np.abs(rp).max()

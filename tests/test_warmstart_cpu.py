@@ -60,3 +60,20 @@ def test_kernel_library_exports_its_header():
     assert "ws_gemm" in names and "ws_adam" in names
     lib = ctypes.CDLL(warmstart.WS_LIB)
     assert not [n for n in names if not hasattr(lib, n)]
+
+
+def test_loss_with_neighbour_term_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    p = rng.normal(size=(2, 12))
+    t = rng.normal(size=(2, 12))
+    loss, g = R.loss_grad(p, t, grid=(3, 4), lam=2.5)
+    for idx in [(0, 0), (0, 5), (1, 11), (1, 6)]:
+        q = p.copy()
+        q[idx] += 1e-6
+        lp, _ = R.loss_grad(q, t, grid=(3, 4), lam=2.5)
+        q[idx] -= 2e-6
+        lm, _ = R.loss_grad(q, t, grid=(3, 4), lam=2.5)
+        assert abs((lp - lm) / 2e-6 - g[idx]) <= 1e-7
+    # a constant shift of a prediction changes nothing
+    l2, _ = R.loss_grad(p + np.array([[3.0], [-1.0]]), t, grid=(3, 4), lam=2.5)
+    assert abs(l2 - loss) <= 1e-12
