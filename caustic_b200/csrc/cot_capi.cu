@@ -36,6 +36,7 @@ struct CotProblemDev {
     double *w = nullptr, *wt = nullptr, *d = nullptr, *mu = nullptr, *mut = nullptr, *fc = nullptr;
     double *wq = nullptr;  // weights of the query entry points, apart from a solve's iterate w
     double *phibar = nullptr;
+    double2 *rbuf = nullptr;  // ring vertices between the cell and integration kernels
     int *nv = nullptr, *ovf_list = nullptr, *ovf_list2 = nullptr, *ovf_count = nullptr;
     int *nbc = nullptr, *nbn = nullptr;        // neighbour cache of the solves
     int *nbc_q = nullptr, *nbn_q = nullptr;    // and of the query entry points
@@ -134,7 +135,7 @@ using namespace cot;
 static void free_problem(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
-                    P.wq, P.fc, P.phibar, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
+                    P.wq, P.fc, P.phibar, P.rbuf, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
                     P.Yv};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -416,6 +417,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.wt, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.wq, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
+    if (e == cudaSuccess) e = A((void **)&P.rbuf, N * 32 * sizeof(double2));
     if (e == cudaSuccess) e = A((void **)&P.d, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mu, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mut, N * 8);
@@ -551,6 +553,7 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.tptr = tptr;
     a.wt = P.wt;
     a.phibar = P.phibar;
+    a.rbuf = P.rbuf;
     a.mu = P.mut;
     a.fc = P.fc;
     a.nv = P.nv;

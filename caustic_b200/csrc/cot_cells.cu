@@ -53,6 +53,7 @@ __shared__ unsigned long long cot_pst[16][16];
 // unordered list of m sites, -(COT_NB_HIDDEN + m) the m sites that hid the
 // cell at the last evaluation
 #define COT_NB_HIDDEN 100
+#define COT_RCAP 32  // ring buffer vertices per cell (the split integration)
 
 // ---------------------------------------------------------------------------
 // bucket and tree plane bounds (per evaluation)
@@ -1546,11 +1547,15 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
     if (lane < nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
     SG.sync();
     CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+    // the solve's path only builds the ring here: k_integrate sums over it
+    // from the ring buffer (two kernels with smaller instruction footprints
+    // than one fused kernel)
+    constexpr bool split = !EXACT;
     if (nv >= 3) {
         if constexpr (EXACT)
             acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
-        else
-            acc = integrate_fast<LPC>(S, nv, pix_geo(g), si, lane);
+        else if (lane < nv)
+            a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.x, P.y);
     }
     PSTAT_CLOCK(t3);
     PSTAT_ADD(2, t3 - t2);
@@ -1592,11 +1597,13 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
         }
     }
     if (lane == 0) {
-        a.mu[i] = acc.mu;
-        // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941);
-        // stored without its -w_i nu_i term, which the reduction adds, so
-        // that nu may change after the cells are built
-        a.fc[i] = -(acc.S - wi * acc.mu);
+        if (!split) {
+            a.mu[i] = acc.mu;
+            // f_i = -w_i nu_i - sum_pix rho (int |x-s_i|^2 - w_i area)   (basic_function.cuh:875-941);
+            // stored without its -w_i nu_i term, which the reduction adds, so
+            // that nu may change after the cells are built
+            a.fc[i] = -(acc.S - wi * acc.mu);
+        }
         a.nv[i] = nv;
         if (a.cen != nullptr) {
             const bool ex = nv >= 3;
@@ -1644,6 +1651,44 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a,
         __syncwarp();
     }
     PSTAT_FLUSH();
+}
+
+// The masses and objective terms of the cells whose rings k_cells_fast left
+// in the ring buffer: one warp per cell, fetched from a counter, the same
+// edge-walk integration as the fused path (so the same sums).  Cells above
+// COT_RCAP vertices are integrated by the large-ring pass instead.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_integrate(CotGeo g, CellsArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    int *fetch = a.ovf_count + 6;
+    while (true) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(fetch, 1);
+        i = __shfl_sync(FULLMASK, i, 0);
+        if (i >= g.n) break;
+        const int nv = a.nv[i];
+        if (nv > COT_RCAP) continue;
+        double mu = 0.0, fcv = 0.0;
+        if (nv >= 3) {
+            if (lane < nv) {
+                const double2 v = a.rbuf[(size_t)i * COT_RCAP + lane];
+                S.X[lane] = v.x;
+                S.Y[lane] = v.y;
+            }
+            __syncwarp();
+            const CellAcc acc = integrate_fast<32>(S, nv, pix_geo(g), g.xy[i], lane);
+            mu = acc.mu;
+            fcv = -(acc.S - a.wt[i] * acc.mu);
+        }
+        if (lane == 0) {
+            a.mu[i] = mu;
+            a.fc[i] = fcv;
+        }
+        __syncwarp();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1917,8 +1962,8 @@ static size_t cells_smem(int maxv, int warps)
 }
 
 #define CELLS_WPB 4
-#define CELLS_MINB 5
-static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0;
+#define CELLS_MINB 6
+static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0, g_blocks_per_smi = 0;
 
 template <bool EXACT, int LPC>
 static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int blocks, cudaStream_t s)
@@ -1939,8 +1984,9 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     // any certificate walk starts from (one round of a 16- or 32-lane segment)
     int lmax = 0;
     while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
-    // ovf_count[0..5]: overflow list sizes and fetch counters; [7]: the ticket
-    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 6);
+    // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
+    // integration kernel's fetch counter, [7]: the tree ticket
+    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 7);
     k_tree_build<<<(nb + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(
         g, a.wt, a.phibar, lmax, reinterpret_cast<unsigned int *>(a.ovf_count + 7));
     c.launches += 2;
@@ -1961,6 +2007,12 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     } else {
         launch_fast<false, 16>(g, a, 0, blocks, s);
         launch_fast<false, 32>(g, a, 1, sms, s);
+        c.launches++;
+    }
+    if (!exact) {
+        const int per_smi = g_blocks_per_smi > 0 ? g_blocks_per_smi : 8;
+        const int bi = std::min((g.n + CELLS_WPB - 1) / CELLS_WPB, sms * per_smi);
+        k_integrate<8><<<bi, 32 * CELLS_WPB, sizeof(FastScratch) * CELLS_WPB, s>>>(g, a);
         c.launches++;
     }
     if (timed) {
@@ -2002,6 +2054,11 @@ void configure_cells_kernels()
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false, 16>, 32 * CELLS_WPB,
                                                       sm16) == cudaSuccess && nb > 0)
         g_blocks_per_sm16 = nb;
+    cudaFuncSetAttribute(k_integrate<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_integrate<8>, 32 * CELLS_WPB, sm32) == cudaSuccess &&
+        nb > 0)
+        g_blocks_per_smi = nb;
 }
 
 }  // namespace cot

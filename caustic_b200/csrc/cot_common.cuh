@@ -131,10 +131,11 @@ struct CellsArgs {
     int *nv;               // per cell ring size out
     int *ovf_list;         // cells whose ring outgrew the first pass
     int *ovf_list2;        // cells whose ring outgrew the second pass
-    int *ovf_count;        // 6 device counters: [0] ovf_list size, [1] first-pass
+    int *ovf_count;        // device counters: [0] ovf_list size, [1] first-pass
                            // fetch, [2] large-ring fetch over ovf_list, [3]
                            // ovf_list2 size, [4] second-pass fetch, [5]
-                           // large-ring fetch over ovf_list2
+                           // large-ring fetch over ovf_list2, [6] integration
+                           // fetch, [7] the bound tree's ticket
     int *nbc;              // cached neighbours, COT_NBC per cell (nullable)
     int *nbn;              // their count per cell (0: none)
     double *cen;           // centroids (nullable)
@@ -145,6 +146,7 @@ struct CellsArgs {
     double solid_light[3]; // light position
     double *splat;         // render output, nx*ny (nullable)
     double splat_scale;    // gray_multiple of the render
+    double2 *rbuf;         // ring vertices of the solve's path, 32 per cell
     double *ring_xy;       // optional fixed-stride ring dump (nullable)
     int *ring_lab;
     int ring_cap;
