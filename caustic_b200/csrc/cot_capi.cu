@@ -37,6 +37,8 @@ struct CotProblemDev {
     double *wq = nullptr;  // weights of the query entry points, apart from a solve's iterate w
     double *phibar = nullptr;
     double2 *rbuf = nullptr;  // ring vertices between the cell and integration kernels
+    int *lbuf = nullptr;      // ring generators between the two ring-building kernels
+    int *cstate = nullptr;    // per-cell state between them
     int *nv = nullptr, *ovf_list = nullptr, *ovf_list2 = nullptr, *ovf_count = nullptr;
     int *nbc = nullptr, *nbn = nullptr;        // neighbour cache of the solves
     int *nbc_q = nullptr, *nbn_q = nullptr;    // and of the query entry points
@@ -135,7 +137,7 @@ using namespace cot;
 static void free_problem(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
-                    P.wq, P.fc, P.phibar, P.rbuf, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
+                    P.wq, P.fc, P.phibar, P.rbuf, P.lbuf, P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
                     P.Yv};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -418,6 +420,8 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.wq, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
     if (e == cudaSuccess) e = A((void **)&P.rbuf, N * 32 * sizeof(double2));
+    if (e == cudaSuccess) e = A((void **)&P.lbuf, N * 32 * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.cstate, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.d, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mu, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.mut, N * 8);
@@ -425,7 +429,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.nv, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.ovf_list, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.ovf_list2, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.ovf_count, 8 * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.ovf_count, 16 * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbc, N * COT_NBC * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbn, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
@@ -447,7 +451,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
-    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 8 * sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 16 * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
@@ -554,6 +558,8 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.wt = P.wt;
     a.phibar = P.phibar;
     a.rbuf = P.rbuf;
+    a.lbuf = P.lbuf;
+    a.cstate = P.cstate;
     a.mu = P.mut;
     a.fc = P.fc;
     a.nv = P.nv;

@@ -1329,20 +1329,25 @@ __device__ __noinline__ RegPoly apply_chunk_cold(RegPoly P, int jl, const double
     return apply_chunk<LPC>(P, jl, sxy, si, wi, wt, lane, S, nearest);
 }
 
-// One cell, worked by one segment of LPC lanes (lane = index in the segment).
-// EXACT = true: the per-pixel path that also yields centroids (with the
-// reference's 1e-10 piece rule) and the render, a whole warp per cell;
-// false: the solver's hot path (masses and objective only).  Rings that
-// outgrow LPC vertices go to olist / ocount for the next pass.
-template <bool EXACT, int LPC>
-__device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, const int i, FastScratch &S,
-                                          int *olist, int *ocount)
+// One cell, worked by one segment of LPC lanes (lane = index in the segment),
+// in three phases: cell_first (the first candidates), cell_walk (the
+// certificate over the bound tree) and cell_finish (integrals or the ring
+// buffer, the next evaluation's cache, the per-cell outputs).  A ring that
+// outgrows LPC vertices has nv = -1 from then on and goes to olist / ocount
+// for the next pass.  EXACT = true: the per-pixel path that also yields
+// centroids (with the reference's 1e-10 piece rule) and the render, a whole
+// warp per cell; false: the solver's hot path (masses and objective only).
+//
+// Phase 1: the domain rectangle clipped by the last evaluation's ring (or
+// neighbours), else by the 3x3 buckets around the site.  cached: the cell
+// had a usable cache (the certificate then skips no window).
+template <int LPC>
+__device__ __forceinline__ RegPoly cell_first(const CotGeo &g, const CellsArgs &a, const int i, const double2 si,
+                                              const double wi, FastScratch &S, bool &cached)
 {
     const Seg<LPC> SG;
     const int lane = SG.sl;
     const double *__restrict__ wt = a.wt;
-    const double2 si = g.xy[i];
-    const double wi = wt[i];
     PSTAT_CLOCK(t0);
     // domain rectangle, CCW, relative to the site
     RegPoly P;
@@ -1356,7 +1361,6 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
         P.c = lane == 0 ? -y0 : (lane == 1 ? x1 : (lane == 2 ? y1 : -x0));
         P.l = -(lane + 1);
     }
-    bool ok = true;
     if (lane == 0) S.kn = -1;
     SG.sync();
     const int bi = g.sbucket[i];
@@ -1369,7 +1373,7 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
     const int nraw = (a.nbn != nullptr) ? a.nbn[i] : 0;
     const bool hidden = nraw < -COT_NB_HIDDEN;
     const int ncache = min(nraw >= 0 ? nraw : (hidden ? -nraw - COT_NB_HIDDEN : -nraw), COT_NBC);
-    bool cached = ncache > 0;
+    cached = ncache > 0;
     if (cached) {
         const int lab = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
         bool direct = false;
@@ -1405,11 +1409,26 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
         const int inc = SG.incl_scan(bcnt);
         P = apply_ranges_cold<LPC>(P, bst, bcnt, inc, i, g.xy, si, wi, wt, lane, S, true);
     }
-    ok = P.nv >= 0;
-    const int win = cached ? -1 : COT_WIN;
     PSTAT_CLOCK(t1);
     PSTAT_ADD(0, t1 - t0);
     PSTAT_ADD(10, cached ? 1 : 0);
+    return P;
+}
+
+// Phase 2: every bucket whose sites could cut the ring is found through the
+// bound tree and its sites are applied.
+template <int LPC>
+__device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a, const int i, const double2 si,
+                                             const double wi, RegPoly P, const bool cached, FastScratch &S)
+{
+    const Seg<LPC> SG;
+    const int lane = SG.sl;
+    const double *__restrict__ wt = a.wt;
+    PSTAT_CLOCK(t1);
+    bool ok = P.nv >= 0;
+    const int bi = g.sbucket[i];
+    const int bu = bi % g.bx, bv = bi / g.bx;
+    const int win = cached ? -1 : COT_WIN;
     // ---- 2. certificate over the bound tree --------------------------------
     const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
     bool brute = false;
@@ -1515,7 +1534,20 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
             ok = P.nv >= 0;
         }
     }
-    if (!ok) {
+    PSTAT_CLOCK(t2);
+    PSTAT_ADD(1, t2 - t1);
+    return P;
+}
+
+// Phase 3: overflow hand-off, or the ring's integrals (EXACT) / the ring
+// buffer (solve path), the next evaluation's cache and the per-cell outputs.
+template <bool EXACT, int LPC>
+__device__ __forceinline__ void cell_finish(const CotGeo &g, const CellsArgs &a, const int i, const double2 si,
+                                            const double wi, RegPoly P, FastScratch &S, int *olist, int *ocount)
+{
+    const Seg<LPC> SG;
+    const int lane = SG.sl;
+    if (P.nv < 0) {
         // ring above LPC vertices: hand the cell to the next pass
         if (lane == 0) {
             const int slot = atomicAdd(ocount, 1);
@@ -1527,7 +1559,6 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
     }
     // ---- 3. integrate the density over the cell --------------------------
     PSTAT_CLOCK(t2);
-    PSTAT_ADD(1, t2 - t1);
     const int nv = P.nv;
     if (nv >= 3) {
         // canonical ring start (smallest edge generator) so the integration
@@ -1624,6 +1655,18 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
     }
 }
 
+template <bool EXACT, int LPC>
+__device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, const int i, FastScratch &S,
+                                          int *olist, int *ocount)
+{
+    const double2 si = g.xy[i];
+    const double wi = a.wt[i];
+    bool cached = false;
+    RegPoly P = cell_first<LPC>(g, a, i, si, wi, S, cached);
+    P = cell_walk<LPC>(g, a, i, si, wi, P, cached, S);
+    cell_finish<EXACT, LPC>(g, a, i, si, wi, P, S, olist, ocount);
+}
+
 // The persistent cell kernel: each warp fetches 32 / LPC cells at a time
 // (one per segment) from a counter, so that large cells leave no tail and the
 // segments of a warp run the same phases together.  pass 0: every cell,
@@ -1648,6 +1691,93 @@ __global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a,
         if (base >= total) break;
         const int slot = base + (int)(threadIdx.x & 31) / LPC;
         if (slot < total) fast_cell<EXACT, LPC>(g, a, pass == 0 ? slot : a.ovf_list[slot], S, olist, ocount);
+        __syncwarp();
+    }
+    PSTAT_FLUSH();
+}
+
+// The solve's path in two launches with smaller instruction footprints than
+// k_cells_fast<.., false, 32>, and the same results: k_cells_first runs
+// phase 1 for every cell and leaves each ring (vertices, edge generators) in
+// the ring buffers; k_cells_walk takes the rings back, rebuilds their edge
+// lines from the generators (the same explicitly rounded site_line /
+// side_line as the clips used, so the same bits) and runs phases 2 and 3.
+// Cells that phase 1 empties or overflows are finished by k_cells_first
+// (cstate < 0); otherwise cstate = nv, plus CST_CACHED for a cached cell.
+#define CST_CACHED 0x100
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cells_first(CotGeo g, CellsArgs a)
+{
+    constexpr int LPC = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x >> 5];
+    PSTAT_INIT();
+    const int lane = threadIdx.x & 31;
+    int *fetch = a.ovf_count + 1;
+    while (true) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(fetch, 1);
+        i = __shfl_sync(FULLMASK, i, 0);
+        if (i >= g.n) break;
+        const double2 si = g.xy[i];
+        const double wi = a.wt[i];
+        bool cached = false;
+        const RegPoly P = cell_first<LPC>(g, a, i, si, wi, S, cached);
+        if (P.nv <= 0) {
+            // emptied (hidden cell) or outgrew 32 vertices: finished here
+            cell_finish<false, LPC>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
+            if (lane == 0) a.cstate[i] = -1;
+        } else {
+            if (lane < P.nv) {
+                a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.x, P.y);
+                a.lbuf[(size_t)i * COT_RCAP + lane] = P.l;
+            }
+            if (lane == 0) a.cstate[i] = P.nv | (cached ? CST_CACHED : 0);
+        }
+        __syncwarp();
+    }
+    PSTAT_FLUSH();
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cells_walk(CotGeo g, CellsArgs a)
+{
+    constexpr int LPC = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x >> 5];
+    PSTAT_INIT();
+    const int lane = threadIdx.x & 31;
+    int *fetch = a.ovf_count + 8;
+    while (true) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(fetch, 1);
+        i = __shfl_sync(FULLMASK, i, 0);
+        if (i >= g.n) break;
+        const int st = a.cstate[i];
+        if (st < 0) continue;
+        const double2 si = g.xy[i];
+        const double wi = a.wt[i];
+        RegPoly P;
+        P.nv = st & 0xff;
+        P.x = P.y = P.a = P.b = P.c = 0.0;
+        P.l = 0;
+        if (lane < P.nv) {
+            const double2 v = a.rbuf[(size_t)i * COT_RCAP + lane];
+            P.x = v.x;
+            P.y = v.y;
+            P.l = a.lbuf[(size_t)i * COT_RCAP + lane];
+            if (P.l >= 0) {
+                double key;
+                site_line(g.xy[P.l], si, a.wt[P.l], wi, P.a, P.b, P.c, key);
+            } else {
+                const double4 box = make_double4(g.pd[0] - si.x, g.pd[1] - si.x, g.pd[2] - si.y, g.pd[3] - si.y);
+                side_line(-P.l - 1, box, P.a, P.b, P.c);
+            }
+        }
+        if (lane == 0) S.kn = -1;
+        __syncwarp();
+        P = cell_walk<LPC>(g, a, i, si, wi, P, (st & CST_CACHED) != 0, S);
+        cell_finish<false, LPC>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
         __syncwarp();
     }
     PSTAT_FLUSH();
@@ -1963,7 +2093,14 @@ static size_t cells_smem(int maxv, int warps)
 
 #define CELLS_WPB 4
 #define CELLS_MINB 6
+#ifndef FIRST_MINB
+#define FIRST_MINB 6  // k_cells_first: blocks per SM its registers are sized for
+#endif
+#ifndef WALK_MINB
+#define WALK_MINB 8   // k_cells_walk (64 registers; 6 blocks measured 2 % slower)
+#endif
 static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0, g_blocks_per_smi = 0;
+static int g_blocks_per_smf = 0, g_blocks_per_smw = 0;
 
 template <bool EXACT, int LPC>
 static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int blocks, cudaStream_t s)
@@ -1985,8 +2122,9 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     int lmax = 0;
     while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
     // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
-    // integration kernel's fetch counter, [7]: the tree ticket
-    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 7);
+    // integration kernel's fetch counter, [7]: the tree ticket (cleared by
+    // k_tree_build itself), [8]: k_cells_walk's fetch counter
+    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 9);
     k_tree_build<<<(nb + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(
         g, a.wt, a.phibar, lmax, reinterpret_cast<unsigned int *>(a.ovf_count + 7));
     c.launches += 2;
@@ -2003,7 +2141,12 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     if (exact) {
         launch_fast<true, 32>(g, a, 0, blocks, s);
     } else if (lpc == 32) {
-        launch_fast<false, 32>(g, a, 0, blocks, s);
+        const int bw = std::min(g.n, sms * (g_blocks_per_smw > 0 ? g_blocks_per_smw : WALK_MINB) * CELLS_WPB);
+        const int bf = std::min(g.n, sms * (g_blocks_per_smf > 0 ? g_blocks_per_smf : FIRST_MINB) * CELLS_WPB);
+        const size_t sm = sizeof(FastScratch) * CELLS_WPB;
+        k_cells_first<FIRST_MINB><<<(bf + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+        k_cells_walk<WALK_MINB><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+        c.launches++;
     } else {
         launch_fast<false, 16>(g, a, 0, blocks, s);
         launch_fast<false, 32>(g, a, 1, sms, s);
@@ -2055,6 +2198,18 @@ void configure_cells_kernels()
                                                       sm16) == cudaSuccess && nb > 0)
         g_blocks_per_sm16 = nb;
     cudaFuncSetAttribute(k_integrate<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_cells_first<FIRST_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_cells_walk<WALK_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_first<FIRST_MINB>, 32 * CELLS_WPB, sm32) ==
+            cudaSuccess &&
+        nb > 0)
+        g_blocks_per_smf = nb;
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_walk<WALK_MINB>, 32 * CELLS_WPB, sm32) ==
+            cudaSuccess &&
+        nb > 0)
+        g_blocks_per_smw = nb;
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_integrate<8>, 32 * CELLS_WPB, sm32) == cudaSuccess &&
         nb > 0)

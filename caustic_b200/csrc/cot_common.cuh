@@ -135,7 +135,8 @@ struct CellsArgs {
                            // fetch, [2] large-ring fetch over ovf_list, [3]
                            // ovf_list2 size, [4] second-pass fetch, [5]
                            // large-ring fetch over ovf_list2, [6] integration
-                           // fetch, [7] the bound tree's ticket
+                           // fetch, [7] the bound tree's ticket, [8] the
+                           // certificate kernel's fetch
     int *nbc;              // cached neighbours, COT_NBC per cell (nullable)
     int *nbn;              // their count per cell (0: none)
     double *cen;           // centroids (nullable)
@@ -147,6 +148,8 @@ struct CellsArgs {
     double *splat;         // render output, nx*ny (nullable)
     double splat_scale;    // gray_multiple of the render
     double2 *rbuf;         // ring vertices of the solve's path, 32 per cell
+    int *lbuf;             // their edge generators between k_cells_first and k_cells_walk
+    int *cstate;           // per cell: ring size (+ cached flag) after phase 1, -1 = finished
     double *ring_xy;       // optional fixed-stride ring dump (nullable)
     int *ring_lab;
     int ring_cap;
