@@ -808,6 +808,15 @@ __device__ double solid_angle_of(const SP &P, int nv, double2 si, double z, cons
     return fabs(ang);
 }
 
+// Position of pixel line c (x0 + c s), one explicitly rounded form for every
+// use: the crossings of an edge, the pixel that a piece lies in and the
+// vertical lines of part (b) all see the same line in the same bits.
+__device__ __forceinline__ double lpos(int c, double s, double x0) { return __fma_rn((double)c, s, x0); }
+
+// Edge parameter t where the edge from p (inverse length component inv)
+// meets the line at X.
+__device__ __forceinline__ double line_t(double X, double p, double inv) { return __dmul_rn(__dsub_rn(X, p), inv); }
+
 // Mass and second moment of the cell, regrouped by Green's theorem.
 // For each pixel p, int over cell ∩ p of g equals the sum over the boundary
 // of cell ∩ p of G dy (dG/dx = g).  Summed over the pixels with their
@@ -815,109 +824,184 @@ __device__ double solid_angle_of(const SP &P, int nv, double2 si, double z, cons
 // cross, each piece weighted by its own pixel's density; plus (b) the
 // vertical pixel lines inside the cell, each segment weighted by the density
 // of the pixel on its left minus the one on its right (horizontal pieces have
-// dy = 0).  (b) also produces the fully covered pixels.  Work is O(pixels)
-// with O(1) each plus O(edge length) per edge -- no per-pixel loop over the
-// edges.  Coordinates are taken relative to the centre of the cell's box for
-// accuracy and shifted to the site at the end.  Used when neither centroids
-// (whose reference rule needs per-pixel areas) nor the render are wanted.
+// dy = 0).  (b) also produces the fully covered pixels.  Coordinates are
+// taken relative to the centre of the cell's box for accuracy and shifted
+// to the site at the end.  Used when neither centroids (whose reference rule
+// needs per-pixel areas) nor the render are wanted.
+//
+// Both parts run one piece per lane.  (a): edge k has 1 + (x lines it
+// crosses) + (y lines it crosses) events (its start, then each crossing);
+// a scan over the edges hands every lane one event, and the piece that
+// starts there ends at the next crossing of either family (found in closed
+// form) or at the edge's end.  The pieces are those of walking each edge
+// from crossing to crossing, with the same parameters.  (b): every
+// (vertical line, pixel row) segment inside the cell, likewise handed out
+// by a scan over the lines.  One lane per edge: rings of up to LPC = 32
+// vertices.
 template <int LPC, class SP>
 __device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, double2 si, int lane)
 {
+    static_assert(LPC == 32, "one lane per edge of a ring of up to 32 vertices");
     const Seg<LPC> W;
     CellAcc acc = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const bool act = lane < nv;
+    const int kn = (lane + 1 >= nv) ? 0 : lane + 1;
+    double px = 0.0, py = 0.0, qx = 0.0, qy = 0.0;
     double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
-    for (int k = lane; k < nv; k += LPC) {
-        int kn = (k + 1 == nv) ? 0 : k + 1;
-        double dx = P.X[kn] - P.X[k], dy = P.Y[kn] - P.Y[k];
-        P.EIX[k] = dx != 0.0 ? 1.0 / dx : 0.0;
-        P.EIY[k] = dy != 0.0 ? 1.0 / dy : 0.0;
-        P.ESL[k] = dx != 0.0 ? dy / dx : 0.0;
-        mnx = fmin(mnx, P.X[k]); mxx = fmax(mxx, P.X[k]);
-        mny = fmin(mny, P.Y[k]); mxy = fmax(mxy, P.Y[k]);
+    if (act) {
+        px = P.X[lane]; py = P.Y[lane]; qx = P.X[kn]; qy = P.Y[kn];
+        const double dx = qx - px, dy = qy - py;
+        P.EIX[lane] = dx != 0.0 ? 1.0 / dx : 0.0;
+        P.EIY[lane] = dy != 0.0 ? 1.0 / dy : 0.0;
+        P.ESL[lane] = dx != 0.0 ? dy / dx : 0.0;
+        mnx = px; mxx = px; mny = py; mxy = py;
     }
     mnx = W.min(mnx); mxx = W.max(mxx); mny = W.min(mny); mxy = W.max(mxy);
     W.sync();
     const double ox = 0.5 * (mnx + mxx), oy = 0.5 * (mny + mxy);  // local origin
     const double cx0 = g.pd0 - si.x, cy0 = g.pd2 - si.y;           // pixel line 0, site frame
     double sA = 0.0, sIa = 0.0, sIb = 0.0, sI2 = 0.0;
-    // (a) edge pieces, one lane per edge
-    for (int k = lane; k < nv; k += LPC) {
-        int kn = (k + 1 == nv) ? 0 : k + 1;
-        const double px = P.X[k], py = P.Y[k], qx = P.X[kn], qy = P.Y[kn];
+
+    // ---- (a) edge pieces --------------------------------------------------
+    // edge `lane`: first x line beyond p and count of x lines strictly
+    // between p and q (cf, nxc), the same for y (rf, nyc)
+    int cf = 0, nxc = 0, rf = 0, nyc = 0, cnt = 0;
+    {
         const double dx = qx - px, dy = qy - py;
-        if (dy == 0.0) continue;  // horizontal: no x-dy term
-        if (dx == 0.0) {
+        bool skip = !act || dy == 0.0;  // horizontal: no x-dy term
+        if (!skip && dx == 0.0) {
             // a vertical edge on a pixel line is counted with the lines in (b)
-            double c = (px - cx0) * g.ixs;
-            int ci = (int)floor(c + 0.5);
-            if ((double)ci * g.xs + cx0 == px) continue;
+            const int ci = (int)floor((px - cx0) * g.ixs + 0.5);
+            if (lpos(ci, g.xs, cx0) == px) skip = true;
         }
-        const double idx = P.EIX[k], idy = P.EIY[k];
-        // crossings with vertical lines X_c and horizontal lines Y_r strictly inside
-        const int cstep = dx > 0.0 ? 1 : -1, rstep = dy > 0.0 ? 1 : -1;
-        int c = (int)floor((px - cx0) * g.ixs) + (dx > 0.0 ? 0 : 1);
-        int r = (int)floor((py - cy0) * g.iys) + (dy > 0.0 ? 0 : 1);
-        auto next_x = [&](void) -> double {
-            if (dx == 0.0) return 2.0;
-            for (int guard = 0; guard < 4; guard++) {
-                double X = (double)c * g.xs + cx0;
-                if (dx > 0.0 ? X >= qx : X <= qx) return 2.0;
-                if (dx > 0.0 ? X > px : X < px) return (X - px) * idx;
-                c += cstep;
-            }
-            return 2.0;
-        };
-        auto next_y = [&](void) -> double {
-            for (int guard = 0; guard < 4; guard++) {
-                double Y = (double)r * g.ys + cy0;
-                if (dy > 0.0 ? Y >= qy : Y <= qy) return 2.0;
-                if (dy > 0.0 ? Y > py : Y < py) return (Y - py) * idy;
-                r += rstep;
-            }
-            return 2.0;
-        };
-        double tx = next_x(), ty = next_y(), tp = 0.0;
-        for (int guard = 0; guard < 4 * (g.nx + g.ny) + 8; guard++) {
-            const double tn = fmin(fmin(tx, ty), 1.0);
-            if (tn > tp) {
-                const double ax = (tp == 0.0 ? px : px + tp * dx), ay = (tp == 0.0 ? py : py + tp * dy);
-                const double bx = (tn == 1.0 ? qx : px + tn * dx), by = (tn == 1.0 ? qy : py + tn * dy);
-                const double tm = 0.5 * (tp + tn);
-                // pixel of the piece, settled against the same line positions
-                // c * xs + x0 that the crossings and part (b) use (the
-                // product form and the quotient form can round apart at the
-                // image's far sides)
-                const double xm = px + tm * dx, ym = py + tm * dy;
-                int ix = (int)floor((xm - cx0) * g.ixs);
-                int iy = (int)floor((ym - cy0) * g.iys);
-                if ((double)ix * g.xs + cx0 > xm) ix--;
-                else if ((double)(ix + 1) * g.xs + cx0 <= xm) ix++;
-                if ((double)iy * g.ys + cy0 > ym) iy--;
-                else if ((double)(iy + 1) * g.ys + cy0 <= ym) iy++;
-                // a piece outside the image (a rounding sliver along the
-                // domain sides) carries no density
-                if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny) {
-                    if (tn >= 1.0) break;
-                    if (tn == tx) { c += cstep; tx = next_x(); }
-                    if (tn == ty) { r += rstep; ty = next_y(); }
-                    tp = tn;
-                    continue;
+        if (!skip) {
+            if (dx != 0.0) {
+                const bool up = dx > 0.0;
+                int c = (int)floor((px - cx0) * g.ixs) + (up ? 0 : 1);
+                for (int gd = 0; gd < 4; gd++) {
+                    const double X = lpos(c, g.xs, cx0);
+                    if (up ? X > px : X < px) break;
+                    c += up ? 1 : -1;
                 }
-                const double rho = g.rho[ix + iy * g.nx];
-                Mom m = {0.0, 0.0, 0.0, 0.0};
-                seg_terms(ax - ox, ay - oy, bx - ox, by - oy, m);
-                sA += rho * m.A;
-                sIa += rho * m.Ia;
-                sIb += rho * m.Ib;
-                sI2 += rho * m.I2;
+                int e = (int)floor((qx - cx0) * g.ixs) + (up ? 0 : 1);  // last line short of q
+                for (int gd = 0; gd < 4; gd++) {
+                    const double X = lpos(e, g.xs, cx0);
+                    if (up ? X < qx : X > qx) break;
+                    e += up ? -1 : 1;
+                }
+                for (int gd = 0; gd < 4; gd++) {
+                    const double X = lpos(e + (up ? 1 : -1), g.xs, cx0);
+                    if (!(up ? X < qx : X > qx)) break;
+                    e += up ? 1 : -1;
+                }
+                cf = c;
+                nxc = max(0, (up ? e - c : c - e) + 1);
             }
-            if (tn >= 1.0) break;
-            if (tn == tx) { c += cstep; tx = next_x(); }
-            if (tn == ty) { r += rstep; ty = next_y(); }
-            tp = tn;
+            {
+                const bool up = dy > 0.0;
+                int r = (int)floor((py - cy0) * g.iys) + (up ? 0 : 1);
+                for (int gd = 0; gd < 4; gd++) {
+                    const double Y = lpos(r, g.ys, cy0);
+                    if (up ? Y > py : Y < py) break;
+                    r += up ? 1 : -1;
+                }
+                int e = (int)floor((qy - cy0) * g.iys) + (up ? 0 : 1);
+                for (int gd = 0; gd < 4; gd++) {
+                    const double Y = lpos(e, g.ys, cy0);
+                    if (up ? Y < qy : Y > qy) break;
+                    e += up ? -1 : 1;
+                }
+                for (int gd = 0; gd < 4; gd++) {
+                    const double Y = lpos(e + (up ? 1 : -1), g.ys, cy0);
+                    if (!(up ? Y < qy : Y > qy)) break;
+                    e += up ? 1 : -1;
+                }
+                rf = r;
+                nyc = max(0, (up ? e - r : r - e) + 1);
+            }
+            cnt = 1 + nxc + nyc;
         }
     }
-    // (b) vertical pixel lines inside the cell
+    {
+        const int inc = W.incl_scan(cnt);
+        const int tot = W.shfl(inc, LPC - 1);
+        for (int base = 0; base < tot; base += LPC) {
+            const int t = base + lane;
+            int k = 0;  // edges whose events end at or before t
+#pragma unroll
+            for (int sft = LPC / 2; sft >= 1; sft >>= 1) {
+                const int v = W.shfl(inc, k + sft - 1);
+                if (v <= t) k += sft;
+            }
+            k &= LPC - 1;
+            const int ik = W.shfl(inc, k), ck = W.shfl(cnt, k);
+            const int kcf = W.shfl(cf, k), knx = W.shfl(nxc, k), krf = W.shfl(rf, k), kny = W.shfl(nyc, k);
+            if (t >= tot) continue;
+            const int m = t - (ik - ck);
+            const int kk = (k + 1 >= nv) ? 0 : k + 1;
+            const double ex = P.X[k], ey = P.Y[k], fx = P.X[kk], fy = P.Y[kk];
+            const double dx = fx - ex, dy = fy - ey;
+            const double idx = P.EIX[k], idy = P.EIY[k];
+            const int cs = dx > 0.0 ? 1 : -1, rs = dy > 0.0 ? 1 : -1;
+            // t of the j-th x / y crossing of the edge
+            auto tx = [&](int j) -> double { return line_t(lpos(kcf + j * cs, g.xs, cx0), ex, idx); };
+            auto ty = [&](int j) -> double { return line_t(lpos(krf + j * rs, g.ys, cy0), ey, idy); };
+            double t0;
+            int jx, jy;  // first x / y crossing after t0
+            bool dup = false;
+            if (m == 0) {
+                t0 = 0.0;
+                jx = 0;
+                jy = 0;
+            } else if (m <= knx) {
+                jx = m;
+                t0 = tx(m - 1);
+                // first y crossing past t0: estimate from the position, then settle
+                const double ym = __fma_rn(t0, dy, ey);
+                int r = (int)floor((ym - cy0) * g.iys) + (rs > 0 ? 1 : 0);
+                jy = min(max((r - krf) * rs, 0), kny);
+                for (int gd = 0; gd < 4 && jy > 0 && ty(jy - 1) > t0; gd++) jy--;
+                for (int gd = 0; gd < 4 && jy < kny && ty(jy) <= t0; gd++) jy++;
+            } else {
+                jy = m - knx;
+                t0 = ty(jy - 1);
+                const double xm = __fma_rn(t0, dx, ex);
+                int c = (int)floor((xm - cx0) * g.ixs) + (cs > 0 ? 1 : 0);
+                jx = knx > 0 ? min(max((c - kcf) * cs, 0), knx) : 0;
+                for (int gd = 0; gd < 4 && jx > 0 && tx(jx - 1) > t0; gd++) jx--;
+                for (int gd = 0; gd < 4 && jx < knx && tx(jx) <= t0; gd++) jx++;
+                // an x crossing at the same t (a pixel corner) owns the piece
+                dup = jx > 0 && tx(jx - 1) == t0;
+            }
+            const double t1 = fmin(fmin(jx < knx ? tx(jx) : 2.0, jy < kny ? ty(jy) : 2.0), 1.0);
+            if (dup || !(t1 > t0)) continue;
+            const double ax = t0 == 0.0 ? ex : __fma_rn(t0, dx, ex), ay = t0 == 0.0 ? ey : __fma_rn(t0, dy, ey);
+            const double bx = t1 == 1.0 ? fx : __fma_rn(t1, dx, ex), by = t1 == 1.0 ? fy : __fma_rn(t1, dy, ey);
+            const double tm = 0.5 * (t0 + t1);
+            // pixel of the piece, settled against the line positions
+            const double xm = __fma_rn(tm, dx, ex), ym = __fma_rn(tm, dy, ey);
+            int ix = (int)floor((xm - cx0) * g.ixs);
+            int iy = (int)floor((ym - cy0) * g.iys);
+            if (lpos(ix, g.xs, cx0) > xm) ix--;
+            else if (lpos(ix + 1, g.xs, cx0) <= xm) ix++;
+            if (lpos(iy, g.ys, cy0) > ym) iy--;
+            else if (lpos(iy + 1, g.ys, cy0) <= ym) iy++;
+            // a piece outside the image (a rounding sliver along the domain
+            // sides) carries no density
+            if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny) continue;
+            const double rho = g.rho[ix + iy * g.nx];
+            Mom mm = {0.0, 0.0, 0.0, 0.0};
+            seg_terms(ax - ox, ay - oy, bx - ox, by - oy, mm);
+            sA += rho * mm.A;
+            sIa += rho * mm.Ia;
+            sIb += rho * mm.Ib;
+            sI2 += rho * mm.I2;
+        }
+    }
+
+    // ---- (b) vertical pixel lines inside the cell --------------------------
+    // pixel columns [lx, hx) and rows [ly, hy) of the cell's box, one pixel
+    // wider on each side; lines lx .. hx
     int lx = (int)floor((mnx - cx0) * g.ixs) - 1;
     int ly = (int)floor((mny - cy0) * g.iys) - 1;
     int hx = (int)floor((mxx - cx0) * g.ixs) + 2;
@@ -926,47 +1010,53 @@ __device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g,
     ly = max(ly, 0);
     hx = min(hx, g.nx);
     hy = min(hy, g.ny);
-    for (int cxs = lx; cxs < hx; cxs += LPC) {
-        const int cw = min(LPC, hx - cxs);
-        for (int c = lane; c <= cw; c += LPC) {
-            double xl = (double)(cxs + c) * g.xs + cx0;
-            double lo, hi;
-            section_at(P, nv, xl, lo, hi);
-            P.elo[c] = lo;
-            P.ehi[c] = hi;
-            P.rv[c] = (mnx <= xl && xl < mxx) ? 1 : 0;  // right limit: left side of a pixel
-            P.lv[c] = (mnx < xl && xl <= mxx) ? 1 : 0;  // left limit: right side of a pixel
-        }
-        W.sync();
-        const int rows = hy - ly, npx = cw * rows;
-        for (int q = lane; q < npx; q += LPC) {
-            const int c = q % cw, rr = q / cw;
-            const int ix = cxs + c, iy = ly + rr;
-            const double y0 = (double)iy * g.ys + cy0, y1 = (double)(iy + 1) * g.ys + cy0;
-            Mom m = {0.0, 0.0, 0.0, 0.0};
-            bool any = false;
-            if (P.lv[c + 1]) {  // right side of the pixel, upwards
-                double b0 = fmax(P.elo[c + 1], y0), b1 = fmin(P.ehi[c + 1], y1);
-                if (b1 > b0) {
-                    vside_terms((double)(ix + 1) * g.xs + cx0 - ox, b0 - oy, b1 - oy, m);
-                    any = true;
+    for (int cxs = lx; cxs <= hx; cxs += LPC) {
+        const int l = cxs + lane;
+        double lo = INFINITY, hi = -INFINITY, xl = 0.0;
+        int r0 = 0, rc = 0;
+        bool fl = false, fr = false;
+        if (l <= hx) {
+            xl = lpos(l, g.xs, cx0);
+            fl = l - 1 >= lx && mnx < xl && xl <= mxx;  // right side of pixel l-1 (a left limit)
+            fr = l < hx && mnx <= xl && xl < mxx;       // left side of pixel l (a right limit)
+            if (fl || fr) {
+                section_at(P, nv, xl, lo, hi);
+                if (hi > lo) {
+                    r0 = max((int)floor((lo - cy0) * g.iys) - 1, ly);
+                    const int r1 = min((int)floor((hi - cy0) * g.iys) + 1, hy - 1);
+                    rc = max(0, r1 - r0 + 1);
                 }
             }
-            if (P.rv[c]) {      // left side, downwards
-                double b0 = fmax(P.elo[c], y0), b1 = fmin(P.ehi[c], y1);
-                if (b1 > b0) {
-                    vside_terms((double)ix * g.xs + cx0 - ox, b1 - oy, b0 - oy, m);
-                    any = true;
-                }
-            }
-            if (!any) continue;
-            const double rho = g.rho[ix + iy * g.nx];
-            sA += rho * m.A;
-            sIa += rho * m.Ia;
-            sIb += rho * m.Ib;
-            sI2 += rho * m.I2;
         }
-        W.sync();
+        const int inc = W.incl_scan(rc);
+        const int tot = W.shfl(inc, LPC - 1);
+        for (int base = 0; base < tot; base += LPC) {
+            const int t = base + lane;
+            int k = 0;
+#pragma unroll
+            for (int sft = LPC / 2; sft >= 1; sft >>= 1) {
+                const int v = W.shfl(inc, k + sft - 1);
+                if (v <= t) k += sft;
+            }
+            k &= LPC - 1;
+            const int ik = W.shfl(inc, k), ck = W.shfl(rc, k), kr0 = W.shfl(r0, k);
+            const double klo = W.shfl(lo, k), khi = W.shfl(hi, k), kxl = W.shfl(xl, k);
+            const bool kfl = W.shfl((int)fl, k) != 0, kfr = W.shfl((int)fr, k) != 0;
+            if (t >= tot) continue;
+            const int r = kr0 + (t - (ik - ck));
+            const double b0 = fmax(klo, lpos(r, g.ys, cy0)), b1 = fmin(khi, lpos(r + 1, g.ys, cy0));
+            if (!(b1 > b0)) continue;
+            const int lk = cxs + k;
+            const double wl = kfl ? g.rho[(lk - 1) + r * g.nx] : 0.0;
+            const double wr = kfr ? g.rho[lk + r * g.nx] : 0.0;
+            Mom mm = {0.0, 0.0, 0.0, 0.0};
+            vside_terms(kxl - ox, b0 - oy, b1 - oy, mm);  // upwards: the left pixel's right side
+            const double wd = wl - wr;
+            sA += wd * mm.A;
+            sIa += wd * mm.Ia;
+            sIb += wd * mm.Ib;
+            sI2 += wd * mm.I2;
+        }
     }
     sA = W.sum(sA);
     sIa = W.sum(sIa);
