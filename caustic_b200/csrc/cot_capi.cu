@@ -348,41 +348,38 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
         if ((int)off.size() >= COT_MAX_LEVELS) return failf(h, COT_EINVAL, "too many tree levels");
     }
     const int nlev = (int)off.size();
+    // per node: the box of its sites {centre x, centre y, half width,
+    // half height}, widened by a relative 1e-12 (an empty node: half width -1)
     std::vector<double4> tst(total);
+    auto boxed = [&](double x0, double x1, double y0, double y1) {
+        const double hx = 0.5 * (x1 - x0) * (1.0 + 1e-12) + 1e-15 * L;
+        const double hy = 0.5 * (y1 - y0) * (1.0 + 1e-12) + 1e-15 * L;
+        return make_double4(0.5 * (x0 + x1), 0.5 * (y0 + y1), hx, hy);
+    };
     for (int b = 0; b < nb; b++) {
-        int s0 = cnt[b], s1 = cnt[b + 1];
-        double mx = 0, my = 0;
-        for (int p = s0; p < s1; p++) { mx += sxy[2 * p]; my += sxy[2 * p + 1]; }
-        int c = s1 - s0;
-        if (c > 0) { mx /= c; my /= c; }
-        double r = 0;
-        for (int p = s0; p < s1; p++) r = std::max(r, std::hypot(sxy[2 * p] - mx, sxy[2 * p + 1] - my));
-        r = r * (1.0 + 1e-12) + 1e-15 * L;
-        tst[b] = make_double4(mx, my, r, (double)c);
+        const int s0 = cnt[b], s1 = cnt[b + 1];
+        if (s1 <= s0) { tst[b] = make_double4(0.0, 0.0, -1.0, -1.0); continue; }
+        double x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
+        for (int p = s0; p < s1; p++) {
+            x0 = std::min(x0, sxy[2 * p]); x1 = std::max(x1, sxy[2 * p]);
+            y0 = std::min(y0, sxy[2 * p + 1]); y1 = std::max(y1, sxy[2 * p + 1]);
+        }
+        tst[b] = boxed(x0, x1, y0, y1);
     }
     for (int l = 1; l < nlev; l++) {
         for (int v = 0; v < lh[l]; v++)
             for (int u = 0; u < lw[l]; u++) {
-                double c = 0, mx = 0, my = 0;
+                double x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
                 for (int bb = 0; bb < 2; bb++)
                     for (int aa = 0; aa < 2; aa++) {
                         int uu = 2 * u + aa, vv = 2 * v + bb;
                         if (uu >= lw[l - 1] || vv >= lh[l - 1]) continue;
-                        double4 ch = tst[off[l - 1] + uu + vv * lw[l - 1]];
-                        c += ch.w; mx += ch.w * ch.x; my += ch.w * ch.y;
+                        const double4 ch = tst[off[l - 1] + uu + vv * lw[l - 1]];
+                        if (ch.z < 0.0) continue;
+                        x0 = std::min(x0, ch.x - ch.z); x1 = std::max(x1, ch.x + ch.z);
+                        y0 = std::min(y0, ch.y - ch.w); y1 = std::max(y1, ch.y + ch.w);
                     }
-                if (c > 0) { mx /= c; my /= c; }
-                double r = 0;
-                for (int bb = 0; bb < 2; bb++)
-                    for (int aa = 0; aa < 2; aa++) {
-                        int uu = 2 * u + aa, vv = 2 * v + bb;
-                        if (uu >= lw[l - 1] || vv >= lh[l - 1]) continue;
-                        double4 ch = tst[off[l - 1] + uu + vv * lw[l - 1]];
-                        if (ch.w <= 0) continue;
-                        r = std::max(r, std::hypot(ch.x - mx, ch.y - my) + ch.z);
-                    }
-                r = r * (1.0 + 1e-12) + 1e-15 * L;
-                tst[off[l] + u + v * lw[l]] = make_double4(mx, my, r, c);
+                tst[off[l] + u + v * lw[l]] = x1 >= x0 ? boxed(x0, x1, y0, y1) : make_double4(0.0, 0.0, -1.0, -1.0);
             }
     }
     // density per unit area, summing to sum(nu) over the domain

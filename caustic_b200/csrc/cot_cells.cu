@@ -94,13 +94,13 @@ __global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const doubl
 }
 
 // Plane bound of bucket b: c_b = slope of phi across the neighbouring buckets
-// (central difference of their means, one-sided at the grid edges), A_b =
-// max_j c_b.s_j - phi_j.
+// (central difference of their mean phi over their box centres, one-sided at
+// the grid edges), A_b = max_j c_b.s_j - phi_j.
 __device__ __forceinline__ void bucket_bound(const CotGeo &g, const double *__restrict__ wt,
                                              const double *__restrict__ phibar, int b)
 {
     const double4 st = g.tstat[b];
-    if (st.w <= 0.0) {
+    if (st.z < 0.0) {
         g.tdyn[b] = make_double4(0.0, 0.0, -INFINITY, 0.0);
         return;
     }
@@ -110,11 +110,11 @@ __device__ __forceinline__ void bucket_bound(const CotGeo &g, const double *__re
     for (int ax = 0; ax < 2; ax++) {
         int bp = -1, bm = -1;
         if (ax == 0) {
-            if (u + 1 < g.bx && g.tstat[b + 1].w > 0.0) bp = b + 1;
-            if (u > 0 && g.tstat[b - 1].w > 0.0) bm = b - 1;
+            if (u + 1 < g.bx && g.tstat[b + 1].z >= 0.0) bp = b + 1;
+            if (u > 0 && g.tstat[b - 1].z >= 0.0) bm = b - 1;
         } else {
-            if (v + 1 < g.by && g.tstat[b + g.bx].w > 0.0) bp = b + g.bx;
-            if (v > 0 && g.tstat[b - g.bx].w > 0.0) bm = b - g.bx;
+            if (v + 1 < g.by && g.tstat[b + g.bx].z >= 0.0) bp = b + g.bx;
+            if (v > 0 && g.tstat[b - g.bx].z >= 0.0) bm = b - g.bx;
         }
         const double mb = ax == 0 ? st.x : st.y;
         double val;
@@ -149,7 +149,7 @@ __device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
     const int W = g.lev_w[L];
     const int node = g.lev_off[L] + q;
     const double4 st = g.tstat[node];
-    if (st.w <= 0.0) {
+    if (st.z < 0.0) {
         g.tdyn[node] = make_double4(0.0, 0.0, -INFINITY, 0.0);
         return;
     }
@@ -162,7 +162,7 @@ __device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
             const int uu = 2 * u + aa, vv = 2 * v + bb;
             if (uu >= cw || vv >= ch) continue;
             const int cn = co + uu + vv * cw;
-            if (g.tstat[cn].w <= 0.0) continue;
+            if (g.tstat[cn].z < 0.0) continue;
             const double4 dy = g.tdyn[cn];
             cx += dy.x;
             cy += dy.y;
@@ -177,10 +177,12 @@ __device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
             if (uu >= cw || vv >= ch) continue;
             const int cn = co + uu + vv * cw;
             const double4 cs = g.tstat[cn];
-            if (cs.w <= 0.0) continue;
+            if (cs.z < 0.0) continue;
             const double4 dy = g.tdyn[cn];
             const double dx = cx - dy.x, dyy = cy - dy.y;
-            A = fmax(A, dy.z + dx * cs.x + dyy * cs.y + sqrt(dx * dx + dyy * dyy) * cs.z);
+            // the child's bound at the parent's slope point c: its plane value
+            // at the box centre plus the box's extent along c - c_child
+            A = fmax(A, dy.z + dx * cs.x + dyy * cs.y + fabs(dx) * cs.z + fabs(dyy) * cs.w);
         }
     g.tdyn[node] = make_double4(cx, cy, A, 0.0);
 }
@@ -510,24 +512,27 @@ __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, dou
     return nv;
 }
 
-// Can no site of `node` beat site i anywhere on the current polygon?
+// Can no site of `node` beat site i anywhere on the current polygon?  For
+// every site j of the node, P_j(x) = x.s_j - phi_j <= A + (x - c).m +
+// |x - c|_x h_x + |x - c|_y h_y (c, A: the node's plane bound, m, h: the
+// centre and half extents of its sites' box); the node is excluded when that
+// stays below P_i - margin at every vertex (a convex bound minus a linear
+// function peaks at a vertex).
 template <class SP>
 __device__ __forceinline__ bool node_excluded(const SP &P, int nv, const CotGeo &g, int node,
                                               double2 si, double halfs2w)
 {
     double4 st = g.tstat[node];
-    if (st.w <= 0.0) return true;
+    if (st.z < 0.0) return true;
     double4 dy = g.tdyn[node];
     double qx = si.x - dy.x, qy = si.y - dy.y;
     double gx = st.x - si.x, gy = st.y - si.y;
     double K = dy.z + qx * st.x + qy * st.y - halfs2w;
-    double r2 = st.z * st.z;
     for (int k = 0; k < nv; k++) {
         double x = P.X[k], y = P.Y[k];
         double R = -g.margin - K - (x * gx + y * gy);
-        if (R <= 0.0) return false;
         double ux = qx + x, uy = qy + y;
-        if (r2 * (ux * ux + uy * uy) >= R * R) return false;
+        if (!(R > fabs(ux) * st.z + fabs(uy) * st.w)) return false;
     }
     return true;
 }

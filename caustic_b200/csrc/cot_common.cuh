@@ -5,7 +5,7 @@
 //   masses    double  nu[n]      same order
 //   buckets   int     bstart[nb+1]  CSR into the sorted sites, row-major
 //             (bucket (u,v) = u + v*bx) over the sites' bounding box
-//   tree      double4 tstat[nodes] {mean x, mean y, radius, count} (static)
+//   tree      double4 tstat[nodes] {box centre x, y, half width, half height} (static; empty: half width -1)
 //             double4 tdyn[nodes]  {cx, cy, A, 0} plane bound (per evaluation)
 //             level 0 = the buckets, each higher level merges 2x2 nodes
 //   density   double  rho[nx*ny] density per unit area, rho[ix + iy*nx]
@@ -35,7 +35,7 @@ struct CotGeo {
     int lev_off[COT_MAX_LEVELS];
     int lev_w[COT_MAX_LEVELS];
     int lev_h[COT_MAX_LEVELS];
-    const double4 *tstat;  // {mx, my, r, count}
+    const double4 *tstat;  // {box centre x, y, half width, half height}; empty: half width < 0
     double4 *tdyn;         // {cx, cy, A, 0}
     const double *rho;     // density per unit area
     int nx, ny;            // pixels along x, along y
