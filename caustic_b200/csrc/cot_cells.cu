@@ -73,6 +73,23 @@ __device__ __forceinline__ double half_phi(double2 s, double wj)
     return __dmul_rn(0.5, __dsub_rn(__fma_rn(s.x, s.x, __dmul_rn(s.y, s.y)), wj));
 }
 
+// The bucket kernels work one bucket per 16-lane segment (a half warp):
+// the segment's lanes take the bucket's sites in turn.
+#define BSEG 16
+__device__ __forceinline__ unsigned bseg_mask() { return 0xffffu << (threadIdx.x & 16); }
+__device__ __forceinline__ double bseg_sum(double v, unsigned m)
+{
+#pragma unroll
+    for (int o = BSEG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o, BSEG);
+    return v;
+}
+__device__ __forceinline__ double bseg_max(double v, unsigned m)
+{
+#pragma unroll
+    for (int o = BSEG / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(m, v, o, BSEG));
+    return v;
+}
+
 // Trial weights of bucket b's sites and their mean phi (0 for an empty
 // bucket).  Block 0 also clears the cell kernels' counters.
 __global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const double *__restrict__ d,
@@ -80,30 +97,31 @@ __global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const doubl
                              double *__restrict__ phibar, int *counters, int ncounters)
 {
     if (blockIdx.x == 0 && (int)threadIdx.x < ncounters) counters[threadIdx.x] = 0;
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= g.bx * g.by) return;
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) / BSEG;
+    const int sl = threadIdx.x & (BSEG - 1);
+    if (b >= g.bx * g.by) return;  // whole segments leave together
+    const unsigned m = bseg_mask();
     const double t = (d != nullptr && tptr != nullptr) ? *tptr : 0.0;
     const int s0 = g.bstart[b], s1 = g.bstart[b + 1];
     double acc = 0.0;
-    for (int j = s0; j < s1; j++) {
+    for (int j = s0 + sl; j < s1; j += BSEG) {
         const double wj = trial_weight(w, d, t, j);
         wt[j] = wj;
         acc = __dadd_rn(acc, half_phi(g.xy[j], wj));
     }
-    phibar[b] = (s1 > s0) ? acc / (double)(s1 - s0) : 0.0;
+    acc = bseg_sum(acc, m);
+    if (sl == 0) phibar[b] = (s1 > s0) ? acc / (double)(s1 - s0) : 0.0;
 }
 
 // Plane bound of bucket b: c_b = slope of phi across the neighbouring buckets
 // (central difference of their mean phi over their box centres, one-sided at
-// the grid edges), A_b = max_j c_b.s_j - phi_j.
-__device__ __forceinline__ void bucket_bound(const CotGeo &g, const double *__restrict__ wt,
-                                             const double *__restrict__ phibar, int b)
+// the grid edges), A_b = max_j c_b.s_j - phi_j.  Called by a whole segment
+// (mask msk); every lane returns the bound.
+__device__ __forceinline__ double4 bucket_bound(const CotGeo &g, const double *__restrict__ wt,
+                                                const double *__restrict__ phibar, int b, int sl, unsigned msk)
 {
     const double4 st = g.tstat[b];
-    if (st.z < 0.0) {
-        g.tdyn[b] = make_double4(0.0, 0.0, -INFINITY, 0.0);
-        return;
-    }
+    if (st.z < 0.0) return make_double4(0.0, 0.0, -INFINITY, 0.0);
     const int u = b % g.bx, v = b / g.bx;
     const double pb = phibar[b];
     double c[2];
@@ -136,14 +154,16 @@ __device__ __forceinline__ void bucket_bound(const CotGeo &g, const double *__re
     }
     double A = -INFINITY;
     const int s0 = g.bstart[b], s1 = g.bstart[b + 1];
-    for (int j = s0; j < s1; j++) {
+    for (int j = s0 + sl; j < s1; j += BSEG) {
         const double2 s = g.xy[j];
         A = fmax(A, c[0] * s.x + c[1] * s.y - half_phi(s, wt[j]));
     }
-    g.tdyn[b] = make_double4(c[0], c[1], A, 0.0);
+    A = bseg_max(A, msk);
+    return make_double4(c[0], c[1], A, 0.0);
 }
 
-// Level L node q = union of up to 2x2 level L-1 nodes.
+// Level L node q = union of up to 2x2 level L-1 nodes.  The children's
+// bounds were written by other blocks of the same launch: read past L1.
 __device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
 {
     const int W = g.lev_w[L];
@@ -155,63 +175,67 @@ __device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
     }
     const int u = q % W, v = q / W;
     const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1], co = g.lev_off[L - 1];
+    double4 cs[4], cd[4];
     double cx = 0.0, cy = 0.0;
     int cnt = 0;
-    for (int bb = 0; bb < 2; bb++)
-        for (int aa = 0; aa < 2; aa++) {
-            const int uu = 2 * u + aa, vv = 2 * v + bb;
-            if (uu >= cw || vv >= ch) continue;
-            const int cn = co + uu + vv * cw;
-            if (g.tstat[cn].z < 0.0) continue;
-            const double4 dy = g.tdyn[cn];
-            cx += dy.x;
-            cy += dy.y;
-            cnt++;
-        }
+    for (int k = 0; k < 4; k++) {
+        cs[k] = make_double4(0.0, 0.0, -1.0, -1.0);
+        cd[k] = make_double4(0.0, 0.0, 0.0, 0.0);
+        const int uu = 2 * u + (k & 1), vv = 2 * v + (k >> 1);
+        if (uu >= cw || vv >= ch) continue;
+        const int cn = co + uu + vv * cw;
+        cs[k] = g.tstat[cn];
+        if (cs[k].z < 0.0) continue;
+        const double2 *dp = reinterpret_cast<const double2 *>(g.tdyn + cn);
+        const double2 d0 = __ldcg(dp), d1 = __ldcg(dp + 1);
+        cd[k] = make_double4(d0.x, d0.y, d1.x, d1.y);
+        cx += cd[k].x;
+        cy += cd[k].y;
+        cnt++;
+    }
     cx /= cnt;
     cy /= cnt;
     double A = -INFINITY;
-    for (int bb = 0; bb < 2; bb++)
-        for (int aa = 0; aa < 2; aa++) {
-            const int uu = 2 * u + aa, vv = 2 * v + bb;
-            if (uu >= cw || vv >= ch) continue;
-            const int cn = co + uu + vv * cw;
-            const double4 cs = g.tstat[cn];
-            if (cs.z < 0.0) continue;
-            const double4 dy = g.tdyn[cn];
-            const double dx = cx - dy.x, dyy = cy - dy.y;
-            // the child's bound at the parent's slope point c: its plane value
-            // at the box centre plus the box's extent along c - c_child
-            A = fmax(A, dy.z + dx * cs.x + dyy * cs.y + fabs(dx) * cs.z + fabs(dyy) * cs.w);
-        }
+    for (int k = 0; k < 4; k++) {
+        if (cs[k].z < 0.0) continue;
+        const double dx = cx - cd[k].x, dyy = cy - cd[k].y;
+        // the child's bound at the parent's slope point c: its plane value
+        // at the box centre plus the box's extent along c - c_child
+        A = fmax(A, cd[k].z + dx * cs[k].x + dyy * cs[k].y + fabs(dx) * cs[k].z + fabs(dyy) * cs[k].w);
+    }
     g.tdyn[node] = make_double4(cx, cy, A, 0.0);
 }
 
-// Bucket plane bounds, then the last block to finish builds tree levels
-// 1..lmax (the levels a certificate walk can start from; the ones above are
-// never read) -- one launch instead of one per level.
+// Bucket plane bounds, one bucket per segment, then the levels 1..lmax (the
+// levels a certificate walk can start from; the ones above are never read)
+// bottom up: every node counts its bounded children on a ticket, and the
+// thread that bounds the last child builds the node, so that no level waits
+// for the whole level below.  Each ticket returns to 0 for the next
+// evaluation once its node is built.
 #define TREE_THREADS 256
 __global__ void __launch_bounds__(TREE_THREADS) k_tree_build(CotGeo g, const double *__restrict__ wt,
-                                                            const double *__restrict__ phibar, int lmax,
-                                                            unsigned int *ticket)
+                                                            const double *__restrict__ phibar, int lmax)
 {
-    __shared__ bool last;
-    const int nb = g.bx * g.by;
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x)
-        bucket_bound(g, wt, phibar, b);
-    if (lmax < 1) return;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) / BSEG;
+    const int sl = threadIdx.x & (BSEG - 1);
+    if (b >= g.bx * g.by) return;  // whole segments leave together
+    const double4 bd = bucket_bound(g, wt, phibar, b, sl, bseg_mask());
+    if (sl != 0) return;
+    g.tdyn[b] = bd;
+    int q = b;
     for (int L = 1; L <= lmax; L++) {
-        const int cnt = g.lev_w[L] * g.lev_h[L];
-        for (int q = threadIdx.x; q < cnt; q += blockDim.x) tree_node(g, L, q);
-        __syncthreads();
+        const int W = g.lev_w[L - 1];
+        const int pu = (q % W) >> 1, pv = (q / W) >> 1;
+        const int pq = pu + pv * g.lev_w[L];
+        const int nch = (2 * pu + 1 < W ? 2 : 1) * (2 * pv + 1 < g.lev_h[L - 1] ? 2 : 1);
+        __threadfence();  // this thread's bound before its ticket
+        const unsigned old = atomicAdd(&g.ttick[g.lev_off[L] + pq], 1u);
+        if ((int)old != nch - 1) return;
+        __threadfence();  // the siblings' bounds after theirs
+        tree_node(g, L, pq);
+        g.ttick[g.lev_off[L] + pq] = 0u;
+        q = pq;
     }
-    if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -2217,11 +2241,10 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     int lmax = 0;
     while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
     // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
-    // integration kernel's fetch counter, [7]: the tree ticket (cleared by
-    // k_tree_build itself), [8]: k_cells_walk's fetch counter
-    k_bucket_phi<<<(nb + 127) / 128, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 9);
-    k_tree_build<<<(nb + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(
-        g, a.wt, a.phibar, lmax, reinterpret_cast<unsigned int *>(a.ovf_count + 7));
+    // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter
+    const int segs = (nb * BSEG + 127) / 128;
+    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 9);
+    k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.phibar, lmax);
     c.launches += 2;
     const int sms = num_sms > 0 ? num_sms : 148;
     const bool exact = a.cen != nullptr || a.splat != nullptr || a.solid != nullptr;

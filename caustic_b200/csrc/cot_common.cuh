@@ -37,6 +37,7 @@ struct CotGeo {
     int lev_h[COT_MAX_LEVELS];
     const double4 *tstat;  // {box centre x, y, half width, half height}; empty: half width < 0
     double4 *tdyn;         // {cx, cy, A, 0}
+    unsigned int *ttick;   // per node: children bounded so far in this evaluation (0 between them)
     const double *rho;     // density per unit area
     int nx, ny;            // pixels along x, along y
     double pd[4];          // proj_domain {xmin, xmax, ymin, ymax}
@@ -135,8 +136,8 @@ struct CellsArgs {
                            // fetch, [2] large-ring fetch over ovf_list, [3]
                            // ovf_list2 size, [4] second-pass fetch, [5]
                            // large-ring fetch over ovf_list2, [6] integration
-                           // fetch, [7] the bound tree's ticket, [8] the
-                           // certificate kernel's fetch
+                           // fetch, [7] unused, [8] the certificate
+                           // kernel's fetch
     int *nbc;              // cached neighbours, COT_NBC per cell (nullable)
     int *nbn;              // their count per cell (0: none)
     double *cen;           // centroids (nullable)
