@@ -1344,14 +1344,12 @@ __device__ __noinline__ RegPoly clip_sides(RegPoly P, double4 box, int lane, Fas
 // lies inside every other line, every edge runs forward along its line and
 // every corner turns left; the ring is then the intersection of those
 // half-planes, with the vertices a sequence of clips would compute (same
-// line pair, same symmetric meet).  Otherwise the result has nv = -2 and
-// the caller clips.  Cuts by sites outside the list are found by the
-// certificate; cuts by domain sides outside it are applied here (nv = -1:
-// the ring grew past LPC vertices).
+// line pair, same symmetric meet).  Otherwise the result has nv = -2, and
+// `backward` marks the lanes whose edge runs backward (a line that no longer
+// reaches the ring, e.g. after an edge flip).
 template <int LPC>
-__device__ __forceinline__ RegPoly ring_from_cache(int lab, int m, const double2 *__restrict__ sxy, double4 box,
-                                                double2 si, double wi, const double *__restrict__ wt, int lane,
-                                                FastScratch &S)
+__device__ __forceinline__ RegPoly ring_try(int lab, int m, const double2 *__restrict__ sxy, double4 box, double2 si,
+                                            double wi, const double *__restrict__ wt, int lane, unsigned &backward)
 {
     const Seg<LPC> W;
     RegPoly P;
@@ -1375,12 +1373,15 @@ __device__ __forceinline__ RegPoly ring_from_cache(int lab, int m, const double2
     }
     const double nvx = W.shfl(vx, nx), nvy = W.shfl(vy, nx);
     const double na = W.shfl(la, nx), nb = W.shfl(lb, nx);
+    bool back = false;
     if (act) {
         // edge k runs along (-b, a) from vertex k to vertex k+1
         const double len = __fma_rn(nvx - vx, -lb, __dmul_rn(nvy - vy, la));
         const double turn = __fma_rn(-lb, na, __dmul_rn(la, nb));
-        if (!(len > 0.0) || !(turn > 0.0)) ok = false;
+        back = !(len > 0.0);
+        if (back || !(turn > 0.0)) ok = false;
     }
+    backward = W.ballot(back);
     if (!W.all(ok)) {
         P.nv = -2;
         return P;
@@ -1392,9 +1393,59 @@ __device__ __forceinline__ RegPoly ring_from_cache(int lab, int m, const double2
     P.c = lc;
     P.l = act ? lab : 0;
     P.nv = m;
+    return P;
+}
+
+// A cached ring that failed its check: drop the generators whose edges run
+// backward and try again (a few times).  Any subset of the cell's true
+// half-planes bounds a superset of the cell, and the certificate walk adds
+// the cuts that are missing, so the result is the same as clipping from the
+// domain rectangle.  nv = -2 when this does not give a valid ring.
+template <int LPC>
+__device__ __noinline__ RegPoly ring_repair(int lab, int m, const double2 *__restrict__ sxy, double4 box, double2 si,
+                                            double wi, const double *__restrict__ wt, int lane, FastScratch &S,
+                                            unsigned backward)
+{
+    const Seg<LPC> W;
+    RegPoly P;
+    P.nv = -2;
+    for (int attempt = 0; attempt < 3 && backward != 0u; attempt++) {
+        const bool keep = lane < m && !((backward >> lane) & 1u);
+        const unsigned km = W.ballot(keep);
+        W.sync();
+        if (keep) S.L[__popc(km & W.below(lane))] = lab;
+        W.sync();
+        m = __popc(km);
+        lab = lane < m ? S.L[lane] : -1;
+        W.sync();
+        if (m < 3) break;
+        P = ring_try<LPC>(lab, m, sxy, box, si, wi, wt, lane, backward);
+        if (P.nv != -2) return P;
+    }
+    P.nv = -2;
+    return P;
+}
+
+// The cached ring rebuilt in one step (ring_try), repaired when generators
+// dropped out.  Cuts by sites outside the list are found by the certificate;
+// cuts by domain sides outside it are applied here (nv = -1: the ring grew
+// past LPC vertices).  nv = -2: the caller clips from the domain rectangle.
+template <int LPC>
+__device__ __forceinline__ RegPoly ring_from_cache(int lab, int m, const double2 *__restrict__ sxy, double4 box,
+                                                double2 si, double wi, const double *__restrict__ wt, int lane,
+                                                FastScratch &S)
+{
+    const Seg<LPC> W;
+    unsigned backward = 0u;
+    RegPoly P = ring_try<LPC>(lab, m, sxy, box, si, wi, wt, lane, backward);
+    if (P.nv == -2) {
+        if (backward == 0u) return P;
+        P = ring_repair<LPC>(lab, m, sxy, box, si, wi, wt, lane, S, backward);
+        if (P.nv == -2) return P;
+    }
     // domain sides that the cell now reaches (rare: clipped out of line)
     bool out = false;
-    if (act) out = vx < box.x || vx > box.y || vy < box.z || vy > box.w;
+    if (lane < P.nv) out = P.x < box.x || P.x > box.y || P.y < box.z || P.y > box.w;
     if (W.any(out)) P = clip_sides<LPC>(P, box, lane, S);
     return P;
 }
