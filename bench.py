@@ -262,8 +262,8 @@ def run_ours(args):
         cell_evals = float(c.item())
     value = cell_evals / (tot_ms * 1e-3)
 
-    # roofline of the cell kernels (ring construction + integration, timed as
-    # one pair per evaluation): CUDA events around every launch need
+    # roofline of the cell kernels (ring construction, certificate and
+    # integration, timed together per evaluation): CUDA events around every launch need
     # the host-driven trial loop (graph-captured launches carry no per-launch
     # events), so one more solve of the same workload runs that way, on the
     # same stream, right after the timed region
@@ -282,7 +282,7 @@ def run_ours(args):
     traffic = committed_traffic()
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
-            "kernel": "k_cells_fast + k_integrate (power-cell rings, then their edge-walk integration; timed as a pair)",
+            "kernel": "k_cells_first + k_cells_walk + k_integrate (power-cell rings, their certificate, their integration; timed together)",
             "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms, "launches": kp["cell_launches"],
             "timing": "CUDA events around each launch, one host-driven solve of the same workload",
             "peak_kind": f"{peak_kind} hbm_gbs (burst copy)"}
