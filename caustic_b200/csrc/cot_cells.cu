@@ -1556,6 +1556,9 @@ __device__ __forceinline__ RegPoly cell_first(const CotGeo &g, const CellsArgs &
             }
         }
         PSTAT_ADD(12, direct ? 1 : 0);
+        PSTAT_ADD(13, (!hidden && nraw < 0) ? 1 : 0);     // unordered cache (long ring)
+        PSTAT_ADD(14, (nraw >= 3 && !direct) ? 1 : 0);    // ordered cache that failed its check
+        PSTAT_ADD(15, hidden ? 1 : 0);
         if (!direct) {
             const int j = (lane < ncache && lab >= 0) ? lab : -1;
             P = apply_chunk_cold<LPC>(P, j, g.xy, si, wi, wt, lane, S, false);

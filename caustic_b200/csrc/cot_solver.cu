@@ -225,13 +225,18 @@ __global__ void __launch_bounds__(32) k_begin_iteration(CotSolver *S)
 {
     __shared__ double G[COT_BASIS * COT_BASIS];
     __shared__ double dl[COT_BASIS];
+    __shared__ double rh[COT_MAX_HIST], alpha[COT_MAX_HIST];
     const int lane = threadIdx.x;
     // only at an iteration boundary: inside a device-driven loop this kernel
     // also runs before every further trial of a line search
     if (S->done || !S->need_begin) return;
     const int m = S->m, B = 2 * m + 1, gi = 2 * m;
+    const int k = S->k;
+    // the control block's arrays once into shared memory: the recursion
+    // below is a chain of 2m dependent steps
     for (int q = lane; q < B * B; q += 32) G[q] = S->G[(q / B) * COT_BASIS + q % B];
     for (int c = lane; c < B; c += 32) dl[c] = (c == gi) ? -1.0 : 0.0;
+    for (int c = lane; c < m; c += 32) rh[c] = S->rho[c];
     __syncwarp();
     auto gdot = [&](int row) -> double {
         double r = 0.0;
@@ -240,24 +245,25 @@ __global__ void __launch_bounds__(32) k_begin_iteration(CotSolver *S)
         for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(FULLMASK, r, o);
         return r;
     };
-    const int cnt = S->k < m ? S->k : m;
+    const int cnt = k < m ? k : m;
     const bool skip = (S->mode == COT_SOLVE_REFERENCE) && S->restart;
-    double alpha[COT_MAX_HIST];
+    const double H0 = S->H0;
     if (!skip) {
         for (int i = 1; i <= cnt; i++) {
-            const int idx = ((S->k - i) % m + m) % m;
-            const double a = gdot(idx) * S->rho[idx];
-            alpha[i - 1] = a;
+            const int idx = ((k - i) % m + m) % m;
+            const double a = gdot(idx) * rh[idx];
             __syncwarp();
-            if (lane == 0) dl[m + idx] -= a;
+            if (lane == 0) {
+                alpha[i - 1] = a;
+                dl[m + idx] -= a;
+            }
             __syncwarp();
         }
-        const double H0 = S->H0;
         for (int c = lane; c < B; c += 32) dl[c] *= H0;
         __syncwarp();
         for (int i = cnt; i > 0; i--) {
-            const int idx = ((S->k - i) % m + m) % m;
-            const double beta = S->rho[idx] * gdot(m + idx);
+            const int idx = ((k - i) % m + m) % m;
+            const double beta = rh[idx] * gdot(m + idx);
             __syncwarp();
             if (lane == 0) dl[idx] += alpha[i - 1] - beta;
             __syncwarp();
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(32) k_begin_iteration(CotSolver *S)
     for (int c = lane; c < COT_BASIS; c += 32) S->delta[c] = c < B ? dl[c] : 0.0;
     if (lane != 0) return;
     if (!skip)
-        for (int i = 1; i <= cnt; i++) S->alpha[((S->k - i) % m + m) % m] = alpha[i - 1];
+        for (int i = 1; i <= cnt; i++) S->alpha[((k - i) % m + m) % m] = alpha[i - 1];
     if (reset) {
         S->k = 0;
         S->H0 = 1.0;
@@ -366,6 +372,21 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
         mu[i] = mt;
     }
     int cnt = initial ? 0 : (S->k + 1 < m ? S->k + 1 : m);  // slots that hold pairs after this update
+    // the new pair and the gradient of this thread's first ACC_REG elements
+    // stay in registers across the m passes below (same sums, same order)
+    constexpr int ACC_REG = 4;
+    double csn[ACC_REG], cyn[ACC_REG], cg[ACC_REG];
+#pragma unroll
+    for (int q = 0; q < ACC_REG; q++) {
+        const int i = b0 + threadIdx.x + q * blockDim.x;
+        csn[q] = cyn[q] = cg[q] = 0.0;
+        if (i < b1) {
+            csn[q] = Sv[(size_t)h * n + i];
+            cyn[q] = Yv[(size_t)h * n + i];
+            cg[q] = mu[i] - nu[i];
+        }
+    }
+    const int brest = b0 + threadIdx.x + ACC_REG * blockDim.x;
     // all 5m+1 sums in one sweep: per-warp partials in shared memory, summed
     // in warp order, then block partials summed in block order by the last
     // block (the order of a per-value block reduction, in one barrier)
@@ -373,7 +394,19 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
         double sy = 0.0, ys = 0.0, yy = 0.0, gs = 0.0, gy = 0.0;
         const int age = ((h - j) % m + m) % m;
         if (cnt > 0 && age < cnt) {
-            for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+#pragma unroll
+            for (int q = 0; q < ACC_REG; q++) {
+                const int i = b0 + threadIdx.x + q * blockDim.x;
+                if (i < b1) {
+                    const double sj = Sv[(size_t)j * n + i], yj = Yv[(size_t)j * n + i];
+                    sy += csn[q] * yj;
+                    ys += cyn[q] * sj;
+                    yy += cyn[q] * yj;
+                    gs += cg[q] * sj;
+                    gy += cg[q] * yj;
+                }
+            }
+            for (int i = brest; i < b1; i += blockDim.x) {
                 double sj = Sv[(size_t)j * n + i], yj = Yv[(size_t)j * n + i];
                 double sn = Sv[(size_t)h * n + i], yn = Yv[(size_t)h * n + i];
                 double g = mu[i] - nu[i];
@@ -398,7 +431,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
         }
     }
     double gg = 0.0;
-    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < ACC_REG; q++)
+        if (b0 + threadIdx.x + q * blockDim.x < b1) gg += cg[q] * cg[q];
+    for (int i = brest; i < b1; i += blockDim.x) {
         double g = mu[i] - nu[i];
         gg += g * g;
     }
