@@ -27,7 +27,6 @@ struct CotProblemDev {
     int *bstart = nullptr;
     int *sbucket = nullptr;
     double4 *tstat = nullptr;
-    unsigned int *ttick = nullptr;  // bound tree build tickets, one per node
     double4 *tdyn = nullptr;
     double *rho = nullptr;
     int *perm = nullptr;   // sorted -> caller index
@@ -137,7 +136,7 @@ using namespace cot;
 
 static void free_problem(CotProblemDev &P)
 {
-    void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.ttick, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
+    void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
                     P.wq, P.fc, P.phibar, P.rbuf, P.lbuf, P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
                     P.Yv};
     for (void *p : ptrs)
@@ -411,7 +410,6 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.sbucket, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.tstat, total * sizeof(double4));
     if (e == cudaSuccess) e = A((void **)&P.tdyn, total * sizeof(double4));
-    if (e == cudaSuccess) e = A((void **)&P.ttick, total * sizeof(unsigned int));
     if (e == cudaSuccess) e = A((void **)&P.rho, rho.size() * 8);
     if (e == cudaSuccess) e = A((void **)&P.perm, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.w, N * 8);
@@ -450,7 +448,6 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
-    COT_CUDA_TRY(cudaMemsetAsync(P.ttick, 0, total * sizeof(unsigned int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 16 * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, N * sizeof(int), s));
@@ -477,7 +474,6 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     }
     g.tstat = P.tstat;
     g.tdyn = P.tdyn;
-    g.ttick = P.ttick;
     g.rho = P.rho;
     g.nx = nx;
     g.ny = ny;

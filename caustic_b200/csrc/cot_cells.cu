@@ -162,80 +162,89 @@ __device__ __forceinline__ double4 bucket_bound(const CotGeo &g, const double *_
     return make_double4(c[0], c[1], A, 0.0);
 }
 
-// Level L node q = union of up to 2x2 level L-1 nodes.  The children's
-// bounds were written by other blocks of the same launch: read past L1.
-__device__ __forceinline__ void tree_node(const CotGeo &g, int L, int q)
-{
-    const int W = g.lev_w[L];
-    const int node = g.lev_off[L] + q;
-    const double4 st = g.tstat[node];
-    if (st.z < 0.0) {
-        g.tdyn[node] = make_double4(0.0, 0.0, -INFINITY, 0.0);
-        return;
-    }
-    const int u = q % W, v = q / W;
-    const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1], co = g.lev_off[L - 1];
-    double4 cs[4], cd[4];
-    double cx = 0.0, cy = 0.0;
-    int cnt = 0;
-    for (int k = 0; k < 4; k++) {
-        cs[k] = make_double4(0.0, 0.0, -1.0, -1.0);
-        cd[k] = make_double4(0.0, 0.0, 0.0, 0.0);
-        const int uu = 2 * u + (k & 1), vv = 2 * v + (k >> 1);
-        if (uu >= cw || vv >= ch) continue;
-        const int cn = co + uu + vv * cw;
-        cs[k] = g.tstat[cn];
-        if (cs[k].z < 0.0) continue;
-        const double2 *dp = reinterpret_cast<const double2 *>(g.tdyn + cn);
-        const double2 d0 = __ldcg(dp), d1 = __ldcg(dp + 1);
-        cd[k] = make_double4(d0.x, d0.y, d1.x, d1.y);
-        cx += cd[k].x;
-        cy += cd[k].y;
-        cnt++;
-    }
-    cx /= cnt;
-    cy /= cnt;
-    double A = -INFINITY;
-    for (int k = 0; k < 4; k++) {
-        if (cs[k].z < 0.0) continue;
-        const double dx = cx - cd[k].x, dyy = cy - cd[k].y;
-        // the child's bound at the parent's slope point c: its plane value
-        // at the box centre plus the box's extent along c - c_child
-        A = fmax(A, cd[k].z + dx * cs[k].x + dyy * cs[k].y + fabs(dx) * cs[k].z + fabs(dyy) * cs[k].w);
-    }
-    g.tdyn[node] = make_double4(cx, cy, A, 0.0);
-}
-
-// Bucket plane bounds, one bucket per segment, then the levels 1..lmax (the
-// levels a certificate walk can start from; the ones above are never read)
-// bottom up: every node counts its bounded children on a ticket, and the
-// thread that bounds the last child builds the node, so that no level waits
-// for the whole level below.  Each ticket returns to 0 for the next
-// evaluation once its node is built.
+// Bucket plane bounds, one bucket per segment.
 #define TREE_THREADS 256
 __global__ void __launch_bounds__(TREE_THREADS) k_tree_build(CotGeo g, const double *__restrict__ wt,
-                                                            const double *__restrict__ phibar, int lmax)
+                                                            const double *__restrict__ phibar)
 {
     const int b = (blockIdx.x * blockDim.x + threadIdx.x) / BSEG;
     const int sl = threadIdx.x & (BSEG - 1);
     if (b >= g.bx * g.by) return;  // whole segments leave together
     const double4 bd = bucket_bound(g, wt, phibar, b, sl, bseg_mask());
-    if (sl != 0) return;
-    g.tdyn[b] = bd;
-    int q = b;
-    for (int L = 1; L <= lmax; L++) {
-        const int W = g.lev_w[L - 1];
-        const int pu = (q % W) >> 1, pv = (q / W) >> 1;
-        const int pq = pu + pv * g.lev_w[L];
-        const int nch = (2 * pu + 1 < W ? 2 : 1) * (2 * pv + 1 < g.lev_h[L - 1] ? 2 : 1);
-        __threadfence();  // this thread's bound before its ticket
-        const unsigned old = atomicAdd(&g.ttick[g.lev_off[L] + pq], 1u);
-        if ((int)old != nch - 1) return;
-        __threadfence();  // the siblings' bounds after theirs
-        tree_node(g, L, pq);
-        g.ttick[g.lev_off[L] + pq] = 0u;
-        q = pq;
+    if (sl == 0) g.tdyn[b] = bd;
+}
+
+// Fixed-order block sum and max over TREE_THREADS threads (every thread
+// gets the result).
+__device__ __forceinline__ double tree_block_sum(double v, double *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULLMASK, v, o);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    for (int k = 0; k < TREE_THREADS / 32; k++) r += sh[k];
+    return r;
+}
+__device__ __forceinline__ double tree_block_max(double v, double *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULLMASK, v, o));
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = -INFINITY;
+    for (int k = 0; k < TREE_THREADS / 32; k++) r = fmax(r, sh[k]);
+    return r;
+}
+
+// Tree levels 1..lmax (the levels a certificate walk can start from; the
+// ones above are never read), one block per node, each straight from the
+// buckets and sites under it: c = the mean slope point of its non-empty
+// buckets, A = max_j c.s_j - phi_j over its sites, the exact value at c.
+// No level waits for the one below, and no bound is a bound of bounds.
+__global__ void __launch_bounds__(TREE_THREADS) k_tree_levels(CotGeo g, const double *__restrict__ wt)
+{
+    __shared__ double sh[TREE_THREADS / 32];
+    const int node = g.lev_off[1] + blockIdx.x;
+    int L = 1;
+    while (L + 1 < g.nlev && g.lev_off[L + 1] <= node) L++;
+    const int q = node - g.lev_off[L], W = g.lev_w[L];
+    if (g.tstat[node].z < 0.0) {
+        if (threadIdx.x == 0) g.tdyn[node] = make_double4(0.0, 0.0, -INFINITY, 0.0);
+        return;
     }
+    // the node's buckets: a rectangle of the bucket grid
+    const int u0 = (q % W) << L, v0 = (q / W) << L;
+    const int u1 = min(u0 + (1 << L), g.bx), v1 = min(v0 + (1 << L), g.by);
+    const int rw = u1 - u0, nbk = rw * (v1 - v0);
+    double sx = 0.0, sy = 0.0, sc = 0.0;
+    for (int k = threadIdx.x; k < nbk; k += TREE_THREADS) {
+        const int b = u0 + k % rw + (v0 + k / rw) * g.bx;
+        if (g.tstat[b].z < 0.0) continue;
+        const double4 d = g.tdyn[b];
+        sx += d.x;
+        sy += d.y;
+        sc += 1.0;
+    }
+    sx = tree_block_sum(sx, sh);
+    sy = tree_block_sum(sy, sh);
+    sc = tree_block_sum(sc, sh);
+    const double cx = sx / sc, cy = sy / sc;
+    double A = -INFINITY;
+    for (int v = v0; v < v1; v++) {
+        // the rectangle's buckets in one row hold consecutive sites
+        const int j0 = g.bstart[u0 + v * g.bx], j1 = g.bstart[u1 + v * g.bx];
+        for (int j = j0 + threadIdx.x; j < j1; j += TREE_THREADS) {
+            const double2 s2 = g.xy[j];
+            A = fmax(A, cx * s2.x + cy * s2.y - half_phi(s2, wt[j]));
+        }
+    }
+    A = tree_block_max(A, sh);
+    if (threadIdx.x == 0) g.tdyn[node] = make_double4(cx, cy, A, 0.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -2298,8 +2307,14 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter
     const int segs = (nb * BSEG + 127) / 128;
     k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 9);
-    k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.phibar, lmax);
+    k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.phibar);
     c.launches += 2;
+    int upper = 0;  // nodes of levels 1..lmax
+    for (int L = 1; L <= lmax; L++) upper += g.lev_w[L] * g.lev_h[L];
+    if (upper > 0) {
+        k_tree_levels<<<upper, TREE_THREADS, 0, s>>>(g, a.wt);
+        c.launches++;
+    }
     const int sms = num_sms > 0 ? num_sms : 148;
     const bool exact = a.cen != nullptr || a.splat != nullptr || a.solid != nullptr;
     const int lpc = (exact || cells_per_warp < 2) ? 32 : 16;

@@ -37,7 +37,6 @@ struct CotGeo {
     int lev_h[COT_MAX_LEVELS];
     const double4 *tstat;  // {box centre x, y, half width, half height}; empty: half width < 0
     double4 *tdyn;         // {cx, cy, A, 0}
-    unsigned int *ttick;   // per node: children bounded so far in this evaluation (0 between them)
     const double *rho;     // density per unit area
     int nx, ny;            // pixels along x, along y
     double pd[4];          // proj_domain {xmin, xmax, ymin, ymax}
