@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cells-per-warp", type=int, default=0, help="1 or 2 (0: the library default)")
     ap.add_argument("--bucket-size", type=int, default=0, help="sites per neighbour bucket (0: the library default)")
+    ap.add_argument("--multilevel", action="store_true",
+                    help="cold against multilevel warm-started solves (config 2, or 5 with --instances)")
+    ap.add_argument("--instances", type=int, default=0, help="instances of a --multilevel run (0: 1, or 16 for config 5)")
     return ap.parse_args()
 
 
@@ -459,10 +462,95 @@ def run_warmstart(args):
     return 0
 
 
+def run_multilevel(args):
+    """Cold solves against multilevel warm-started solves
+    (caustic_b200/multilevel.py) of the same seeded instances to max-rel
+    1e-4, each arm as one batched solve per level.  A step solves every
+    instance once in each arm; the reported value is the multilevel arm's
+    device time per solve (all levels).  Wall times add the host work
+    (problem uploads, coarsening, interpolation)."""
+    import time
+
+    import numpy as np
+    import torch
+
+    from caustic_b200 import capi, multilevel, problems
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    cfg = args.config if args.config in (2, 5) else 2
+    count = args.instances or (16 if cfg == 5 else 1)
+    probs = [problems.make(cfg, i) for i in range(count)]
+
+    def cold_arm(ps):
+        t0 = time.perf_counter()
+        sols = []
+        for p in ps:
+            s = capi.Solver()
+            s.set_problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+            sols.append(s)
+        _, st = capi.solve_batch(sols, [np.zeros(p.n) for p in ps], tol=args.tol, history=args.history,
+                                 max_iter=100000)
+        for s in sols:
+            s.close()
+        return st, st[0].ms, time.perf_counter() - t0
+
+    def ml_arm(ps):
+        t0 = time.perf_counter()
+        _, levels = multilevel.solve(ps, tol=args.tol, history=args.history)
+        return levels, sum(lv.ms for lv in levels), time.perf_counter() - t0
+
+    small = [problems.make(cfg, 900 + i, g=64, res=256) for i in range(2)]
+    for _ in range(args.warmup):
+        cold_arm(small)
+        ml_arm(small)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    tot = {"cold_ms": 0.0, "ml_ms": 0.0, "cold_wall": 0.0, "ml_wall": 0.0}
+    cold_st, ml_lv = [], None
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            torch.cuda.synchronize()
+            st, ms, wall = cold_arm(probs)
+            tot["cold_ms"] += ms
+            tot["cold_wall"] += wall
+            cold_st += st
+            flush.fill_((k + 1) & 255)
+            torch.cuda.synchronize()
+            lv, ms, wall = ml_arm(probs)
+            tot["ml_ms"] += ms
+            tot["ml_wall"] += wall
+            ml_lv = lv
+    n = count * args.steps
+    line = {"metric": "OT solve ms @1e-4 mass err: multilevel warm start vs plain L-BFGS", "impl": "ours",
+            "value": tot["ml_ms"] / n, "unit": "ms/solve", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64 jittered sites + Gaussian-mixture targets)",
+            "config": {"workload": f"sdot_config{cfg}_multilevel_vs_cold", "n_sites": probs[0].n,
+                       "image": list(probs[0].size), "instances": count, "batched": count > 1,
+                       "stop": "max_rel_mass_err<=1e-4", "coarse_stop": "max_rel_mass_err<=1e-3",
+                       "l2": "256 MiB buffer written before each arm"},
+            "cold_ms_per_solve": tot["cold_ms"] / n, "multilevel_ms_per_solve": tot["ml_ms"] / n,
+            "speedup": tot["cold_ms"] / tot["ml_ms"],
+            "cold_wall_ms_per_solve": 1e3 * tot["cold_wall"] / n,
+            "multilevel_wall_ms_per_solve": 1e3 * tot["ml_wall"] / n,
+            "wall_speedup": tot["cold_wall"] / tot["ml_wall"],
+            "cold_iterations_mean": float(np.mean([s.iterations for s in cold_st])),
+            "cold_max_rel_err": float(max(s.max_rel_err for s in cold_st)),
+            "levels": [{"n_sites": lv.n, "image": list(lv.image), "tol": lv.tol, "ms": lv.ms,
+                        "iterations_mean": float(np.mean([s.iterations for s in lv.stats])),
+                        "max_rel_err": float(max(s.max_rel_err for s in lv.stats))} for lv in ml_lv],
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.multilevel:
+        return run_multilevel(args)
     if args.config == 3:
         return run_batch(args)
     if args.config == 4:

@@ -1,0 +1,130 @@
+"""Multilevel warm start for the SDOT solve.
+
+The dual weights are a smooth function of the site position (w(s) =
+|s|^2 - 2 phi(s) for the transport's convex potential phi), so a coarse
+problem carries most of their large-scale shape.  ``solve`` builds a chain
+of problems, each with 2 x 2 sites merged into one (mean position, summed
+mass) and, where the image is fine enough, 2 x 2 pixels merged too.  It
+solves the coarsest from w = 0, then each finer one from the weights of
+the level below, interpolated bilinearly at its sites, and the finest to
+the requested tolerance.  Every level is a plain solve of this library
+(cot_solve / cot_solve_batch), so the plain method remains the judge of
+the error.  The reference has no counterpart: its solver starts from the
+previous weights or zero (main.cu:193-198).
+
+Sites must form a jittered G_x x G_y lattice (``SDOTProblem.grid``), indexed
+i = a + G_x b, as the benchmark problems are.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from .problems import SDOTProblem
+
+
+def coarsen(p: SDOTProblem, min_pixels_per_site: int = 8) -> SDOTProblem:
+    """The problem with each 2 x 2 block of sites merged (mean position,
+    summed mass).  The image is merged 2 x 2 as well (pixel masses summed)
+    while it keeps at least ``min_pixels_per_site`` pixels across a coarse
+    site's pitch, so that a coarse evaluation costs less."""
+    gx, gy = p.grid
+    if gx % 2 or gy % 2:
+        raise ValueError(f"coarsen: site lattice {gx}x{gy} is not even")
+    xy = p.xy.reshape(gy // 2, 2, gx // 2, 2, 2).mean(axis=(1, 3)).reshape(-1, 2)
+    nu = p.nu.reshape(gy // 2, 2, gx // 2, 2).sum(axis=(1, 3)).ravel()
+    W, H = p.size
+    pic, size = p.picture, p.size
+    if W % 2 == 0 and H % 2 == 0 and W // (gx // 2) >= min_pixels_per_site and H // (gy // 2) >= min_pixels_per_site:
+        pic = np.asarray(p.picture, np.float64).reshape(H // 2, 2, W // 2, 2).sum(axis=(1, 3)).ravel()
+        size = (W // 2, H // 2)
+    return SDOTProblem(p.name + "/coarse", xy, nu, pic, size, np.array(p.proj_domain, np.float64), (gx // 2, gy // 2))
+
+
+def prolong(wc: np.ndarray, coarse: SDOTProblem, fine: SDOTProblem) -> np.ndarray:
+    """Weights of ``coarse`` interpolated bilinearly at the sites of
+    ``fine`` (coarse site (a, b) taken at its lattice point ((a + 0.5) / G_x,
+    (b + 0.5) / G_y) of the domain; held constant beyond the outer sites),
+    with their mean removed."""
+    gxc, gyc = coarse.grid
+    Wc = np.asarray(wc, np.float64).reshape(gyc, gxc)
+    d = np.asarray(fine.proj_domain, np.float64)
+    ux = (fine.xy[:, 0] - d[0]) / (d[1] - d[0])
+    uy = (fine.xy[:, 1] - d[2]) / (d[3] - d[2])
+    x = np.clip(ux * gxc - 0.5, 0.0, gxc - 1.0)
+    y = np.clip(uy * gyc - 0.5, 0.0, gyc - 1.0)
+    x0 = np.minimum(np.floor(x).astype(np.int64), max(gxc - 2, 0))
+    y0 = np.minimum(np.floor(y).astype(np.int64), max(gyc - 2, 0))
+    x1 = np.minimum(x0 + 1, gxc - 1)
+    y1 = np.minimum(y0 + 1, gyc - 1)
+    fx, fy = x - x0, y - y0
+    w = (Wc[y0, x0] * (1 - fx) * (1 - fy) + Wc[y0, x1] * fx * (1 - fy) + Wc[y1, x0] * (1 - fx) * fy
+         + Wc[y1, x1] * fx * fy)
+    return w - w.mean()
+
+
+def chain(p: SDOTProblem, min_sites: int = 1024, max_levels: int = 8) -> list:
+    """[p, coarser, ...]: halve the lattice while both sides stay even and
+    the next level keeps at least ``min_sites`` sites."""
+    out = [p]
+    while len(out) <= max_levels:
+        gx, gy = out[-1].grid
+        if gx % 2 or gy % 2 or (gx // 2) * (gy // 2) < min_sites:
+            break
+        out.append(coarsen(out[-1]))
+    return out
+
+
+@dataclass
+class LevelStats:
+    n: int                  # sites of the level
+    image: tuple            # its image size
+    tol: float              # the max-rel error it was solved to
+    stats: list = field(default_factory=list)   # SolveStats of each instance
+    ms: float = 0.0         # device time of the level's (batched) solve
+
+
+def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float = 1e-3, min_sites: int = 1024,
+          history: int = 10, max_iter: int = 100000, w0: Sequence[np.ndarray] = None, batched: bool = True):
+    """Solve every problem to max-rel error ``tol`` through its multilevel
+    chain: the coarsest level from zero (or from ``w0``, one start vector
+    per problem of the coarsest level's size), every other level from the
+    level below, the coarse levels to ``coarse_tol``.  The problems' chains
+    are cut to the shortest one.  Each level runs as one batched solve
+    (cot_solve_batch) when ``batched``, else one solve per problem.
+    Returns (weights of the finest level per problem, [LevelStats] from the
+    coarsest level up); a level's ``ms`` is its device time."""
+    from . import capi
+
+    chains = [chain(p, min_sites) for p in probs]
+    depth = min(len(c) for c in chains)
+    chains = [c[:depth] for c in chains]
+    ws = list(w0) if w0 is not None else [np.zeros(c[-1].n) for c in chains]
+    levels = []
+    for k in range(depth - 1, -1, -1):
+        level = [c[k] for c in chains]
+        if k < depth - 1:
+            ws = [prolong(w, c[k + 1], c[k]) for w, c in zip(ws, chains)]
+        lt = tol if k == 0 else coarse_tol
+        sols = []
+        for q in level:
+            s = capi.Solver()
+            s.set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
+            sols.append(s)
+        try:
+            if batched:
+                ws, st = capi.solve_batch(sols, ws, tol=lt, history=history, max_iter=max_iter)
+                ms = st[0].ms
+            else:
+                res = [s.solve(w, mode=capi.SOLVE_WOLFE, tol=lt, history=history, max_iter=max_iter)
+                       for s, w in zip(sols, ws)]
+                ws = [r[0] for r in res]
+                st = [r[1] for r in res]
+                ms = float(sum(x.ms for x in st))
+        finally:
+            for s in sols:
+                s.close()
+        levels.append(LevelStats(level[0].n, tuple(level[0].size), lt, list(st), ms))
+    return ws, levels
