@@ -56,8 +56,9 @@ def parse():
     ap.add_argument("--cells-per-warp", type=int, default=0, help="1 or 2 (0: the library default)")
     ap.add_argument("--bucket-size", type=int, default=0, help="sites per neighbour bucket (0: the library default)")
     ap.add_argument("--multilevel", action="store_true",
-                    help="cold against multilevel warm-started solves (config 2, or 5 with --instances)")
-    ap.add_argument("--instances", type=int, default=0, help="instances of a --multilevel run (0: 1, or 16 for config 5)")
+                    help="cold against multilevel warm-started solves (config 2, 4 or 5)")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="instances of a --multilevel run (0: 1 at config 2, 64 at config 4, 16 at config 5)")
     return ap.parse_args()
 
 
@@ -478,9 +479,11 @@ def run_multilevel(args):
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    cfg = args.config if args.config in (2, 5) else 2
-    count = args.instances or (16 if cfg == 5 else 1)
-    probs = [problems.make(cfg, i) for i in range(count)]
+    cfg = args.config if args.config in (2, 4, 5) else 2
+    count = args.instances or {2: 1, 4: 64, 5: 16}[cfg]
+    # config 4: the learned warm start's held-out seeds
+    first = 100000 if cfg == 4 else 0
+    probs = [problems.make(cfg, first + i) for i in range(count)]
 
     def cold_arm(ps):
         t0 = time.perf_counter()
