@@ -278,7 +278,9 @@ int main(int argc, char *argv[])
     std::vector<int> idx[4];
     if (!read_pairs(seed + "points.txt", points) || !read_pairs(seed + "proj_xy.txt", proj_xy)) return 5;
     const char *idx_names[4] = {"left_idx.txt", "right_idx.txt", "bottom_idx.txt", "top_idx.txt"};
-    for (int k = 0; k < 4; k++) read_ints(seed + idx_names[k], idx[k]);  // mirrors are not needed
+    // read for the reference's input checks only: cells are built inside
+    // proj_domain directly, so no mirror sites are needed
+    for (int k = 0; k < 4; k++) read_ints(seed + idx_names[k], idx[k]);
     const int n = (int)(points.size() / 2);
     if (n <= 0 || proj_xy.size() != points.size()) {
         std::cerr << "points.txt and proj_xy.txt must hold the same number of sites" << std::endl;

@@ -4,8 +4,8 @@ A convolutional encoder-decoder (U-Net, ``levels`` levels of two 3x3
 convolutions with ReLU, channels ``base * 2**l``) maps a target image and the
 site layout to initial dual weights on the site grid.  The plain L-BFGS
 (``capi.Solver.solve``) then runs from them to the same tolerance: the
-network only moves the starting point, the solver stays the judge of the
-error.
+network only moves the starting point; the solver alone decides when the
+error is small enough.
 
 Every layer runs on the kernels of ``libcausticws.so`` (include/causticws.h):
 im2col + a BF16 tensor-core GEMM with FP32 accumulation for the convolutions,
