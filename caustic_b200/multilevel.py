@@ -9,8 +9,8 @@ solves the coarsest from w = 0, then each finer one from the weights of
 the level below, interpolated bilinearly at its sites, and the finest to
 the requested tolerance.  Every level is a plain solve of this library
 (cot_solve / cot_solve_batch), so the plain method alone decides when the
-error is small enough.  The reference has no counterpart: its solver starts from the
-previous weights or zero (main.cu:193-198).
+error is small enough.  The reference has no counterpart: its solver starts
+from the previous weights or zero (main.cu:193-198).
 
 Sites must form a jittered G_x x G_y lattice (``SDOTProblem.grid``), indexed
 i = a + G_x b, as the benchmark problems are.
