@@ -82,6 +82,8 @@ __device__ double block_reduce(double v, double *sh)
     return sh[32];
 }
 
+#define COT_F_NOISE 1e-12  // relative noise of the objective the line search tolerates
+
 // Line-search decision for the trial just reduced (one thread).
 __device__ void ls_decide(CotSolver *S, const CotEvalOut &o)
 {
@@ -112,7 +114,14 @@ __device__ void ls_decide(CotSolver *S, const CotEvalOut &o)
     double t = S->t;
     bool bad = o.overflow > 0;
     if (bad) S->ring_rejects++;
-    if (bad || !(o.f <= S->f + S->c1 * t * S->gd) || o.f >= S->f_lo) {
+    // approximate Wolfe (Hager and Zhang): near convergence the objective's
+    // evaluation noise (rounding in every cell's terms, about 1e-16 of |f|
+    // per cell) exceeds the decrease a step can still make, and comparisons
+    // of f stop telling steps apart.  A change of f within COT_F_NOISE |f|
+    // is then not held against the step, provided the slope at the trial
+    // point g(t).d <= (2 c1 - 1) g.d: the directional derivative decides.
+    const bool approx = o.f <= S->f + COT_F_NOISE * fabs(S->f) && o.gtd <= (2.0 * S->c1 - 1.0) * S->gd;
+    if (bad || (!approx && (!(o.f <= S->f + S->c1 * t * S->gd) || o.f >= S->f_lo))) {
         S->hi = t;
     } else if (fabs(o.gtd) <= S->c2 * fabs(S->gd)) {
         S->accepted = 1;

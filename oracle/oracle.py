@@ -481,15 +481,19 @@ def max_rel_error(mu, nu):
     return float(np.max(np.abs(mu - nu) / nu))
 
 
+F_NOISE = 1e-12  # relative objective noise the Wolfe search tolerates (COT_F_NOISE)
+
+
 def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0.9,
                 max_ls=30, max_ring=None, max_evals=None):
     """L-BFGS with a strong-Wolfe line search and the max-relative mass stop.
 
     Same rules as the device solver (caustic_b200 csrc/cot_solver.cu):
     first trial step 1 (unit step on the scaled direction), bracketing by
-    doubling, zoom by bisection; the history pair is stored only when
-    y.s > 0; the stop test max_i |mu_i - nu_i| / nu_i <= tol is taken at the
-    accepted point.
+    doubling, zoom by bisection; a change of f within F_NOISE |f| is not
+    held against a step whose slope is small enough (approximate Wolfe); the
+    history pair is stored only when y.s > 0; the stop test
+    max_i |mu_i - nu_i| / nu_i <= tol is taken at the accepted point.
     """
     w = _f64(w0).copy()
     n = w.shape[0]
@@ -542,7 +546,11 @@ def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0
             st.evaluations += 1
             bad = max_ring is not None and e.max_len > max_ring
             gtd = float(e.g @ d)
-            if bad or e.f > f + c1 * t * gd or e.f >= f_lo:
+            # approximate Wolfe (cot_solver.cu ls_decide): a change of f
+            # within F_NOISE |f| (evaluation noise) does not count against
+            # the step when the slope g(t).d <= (2 c1 - 1) g.d
+            approx = e.f <= f + F_NOISE * abs(f) and gtd <= (2.0 * c1 - 1.0) * gd
+            if bad or (not approx and (e.f > f + c1 * t * gd or e.f >= f_lo)):
                 hi = t
             elif abs(gtd) <= c2 * abs(gd):
                 acc = (t, e)
