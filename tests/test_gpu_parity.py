@@ -184,6 +184,16 @@ def test_wolfe_solve_matches_oracle(gpu):
     assert O.max_rel_error(O.evaluate(oracle_problem(p), w).mu, p.nu) <= 1e-4
 
 
+def test_wolfe_solve_passes_the_evaluation_noise_floor(gpu):
+    """The device line search tolerates the objective's evaluation noise as
+    the oracle does (approximate Wolfe): a small problem solves to 1e-10."""
+    p = problems.make(2, 0, g=8, res=32)
+    s = solver_for(p)
+    w, st = s.solve(np.zeros(p.n), mode=capi.SOLVE_WOLFE, tol=1e-10, history=10, max_iter=3000)
+    assert st.converged and st.max_rel_err <= 1e-10
+    assert O.max_rel_error(O.evaluate(oracle_problem(p), w).mu, p.nu) <= 1e-9
+
+
 def test_reference_mode_solve_matches_oracle(gpu):
     """direct_ot's loop (backtracking, stale ||g|| stop) against its restatement."""
     p = problems.make(1, g=12, res=48)

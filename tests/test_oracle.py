@@ -160,6 +160,20 @@ def test_wolfe_solver_reaches_max_relative_tolerance():
     assert O.max_rel_error(O.evaluate(prob, w).mu, p.nu) <= 1e-4
 
 
+def test_wolfe_solver_passes_the_evaluation_noise_floor(monkeypatch):
+    """Near convergence the objective's evaluation noise exceeds what a step
+    can still gain; with the approximate Wolfe rule the solve goes on to
+    1e-10, without it (F_NOISE = 0) it stalls after 50 failed searches."""
+    p = problems.make(2, 0, g=8, res=32)
+    prob = O.Problem(p.xy, p.nu, p.picture, np.array(p.size), p.proj_domain)
+    w, st = O.lbfgs_wolfe(prob, np.zeros(p.n), tol=1e-10, max_iter=3000)
+    assert st.converged and st.restarts == 0
+    assert O.max_rel_error(O.evaluate(prob, w).mu, p.nu) <= 1e-10
+    monkeypatch.setattr(O, "F_NOISE", 0.0)
+    _, st0 = O.lbfgs_wolfe(prob, np.zeros(p.n), tol=1e-10, max_iter=3000)
+    assert not st0.converged and st0.restarts > 50
+
+
 def test_green_integral_is_exact_second_moment():
     """Polygon_Ints (basic_function.cuh:826-865) = int |x - s|^2 for CCW rings."""
     L = O.lib()
