@@ -109,11 +109,10 @@ def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float 
             ws = [prolong(w, c[k + 1], c[k]) for w, c in zip(ws, chains)]
         lt = tol if k == 0 else coarse_tol
         sols = []
-        for q in level:
-            s = capi.Solver()
-            s.set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
-            sols.append(s)
         try:
+            for q in level:
+                sols.append(capi.Solver())
+                sols[-1].set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
             if batched:
                 ws, st = capi.solve_batch(sols, ws, tol=lt, history=history, max_iter=max_iter)
                 ms = st[0].ms
