@@ -86,8 +86,31 @@ class LevelStats:
     ms: float = 0.0         # device time of the level's (batched) solve
 
 
+def _library_level(level, starts, tol, history, max_iter, batched):
+    """One level with this library's solver: (weights, SolveStats list,
+    device ms)."""
+    from . import capi
+
+    sols = []
+    try:
+        for q in level:
+            sols.append(capi.Solver())
+            sols[-1].set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
+        if batched:
+            ws, st = capi.solve_batch(sols, starts, tol=tol, history=history, max_iter=max_iter)
+            return ws, st, st[0].ms
+        res = [s.solve(w, mode=capi.SOLVE_WOLFE, tol=tol, history=history, max_iter=max_iter)
+               for s, w in zip(sols, starts)]
+        st = [r[1] for r in res]
+        return [r[0] for r in res], st, float(sum(x.ms for x in st))
+    finally:
+        for s in sols:
+            s.close()
+
+
 def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float = 1e-3, min_sites: int = 1024,
-          history: int = 10, max_iter: int = 100000, w0: Sequence[np.ndarray] = None, batched: bool = True):
+          history: int = 10, max_iter: int = 100000, w0: Sequence[np.ndarray] = None, batched: bool = True,
+          level_solver=None):
     """Solve every problem to max-rel error ``tol`` through its multilevel
     chain: the coarsest level from zero (or from ``w0``, one start vector
     per problem of the coarsest level's size), every other level from the
@@ -95,9 +118,11 @@ def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float 
     are cut to the shortest one.  Each level runs as one batched solve
     (cot_solve_batch) when ``batched``, else one solve per problem.
     Returns (weights of the finest level per problem, [LevelStats] from the
-    coarsest level up); a level's ``ms`` is its device time."""
-    from . import capi
+    coarsest level up); a level's ``ms`` is its device time.
 
+    ``level_solver(problems, starts, tol)``, when given, solves a level in
+    place of this library's solver and returns (weights, stats with
+    ``iterations`` and ``max_rel_err``, ms)."""
     chains = [chain(p, min_sites) for p in probs]
     depth = min(len(c) for c in chains)
     chains = [c[:depth] for c in chains]
@@ -108,22 +133,9 @@ def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float 
         if k < depth - 1:
             ws = [prolong(w, c[k + 1], c[k]) for w, c in zip(ws, chains)]
         lt = tol if k == 0 else coarse_tol
-        sols = []
-        try:
-            for q in level:
-                sols.append(capi.Solver())
-                sols[-1].set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
-            if batched:
-                ws, st = capi.solve_batch(sols, ws, tol=lt, history=history, max_iter=max_iter)
-                ms = st[0].ms
-            else:
-                res = [s.solve(w, mode=capi.SOLVE_WOLFE, tol=lt, history=history, max_iter=max_iter)
-                       for s, w in zip(sols, ws)]
-                ws = [r[0] for r in res]
-                st = [r[1] for r in res]
-                ms = float(sum(x.ms for x in st))
-        finally:
-            for s in sols:
-                s.close()
+        if level_solver is None:
+            ws, st, ms = _library_level(level, ws, lt, history, max_iter, batched)
+        else:
+            ws, st, ms = level_solver(level, ws, lt)
         levels.append(LevelStats(level[0].n, tuple(level[0].size), lt, list(st), ms))
     return ws, levels

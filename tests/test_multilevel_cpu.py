@@ -57,3 +57,33 @@ def test_prolong_reproduces_linear_functions_inside():
               (p.xy[:, 1] > 0.5 / gy) & (p.xy[:, 1] < 1 - 0.5 / gy))
     d = (w - f(p.xy))[inside]           # a constant: the removed mean
     assert np.ptp(d) < 1e-12
+
+
+def test_multilevel_chain_with_the_oracle_as_level_solver():
+    """The whole chain on the CPU, each level solved by the oracle's Wolfe
+    L-BFGS: the finest level reaches the tolerance and needs fewer
+    iterations than a cold solve of the same problem."""
+    from types import SimpleNamespace
+
+    from oracle import oracle as O
+
+    def oprob(q):
+        return O.Problem(q.xy, q.nu, q.picture, np.array(q.size), q.proj_domain)
+
+    def level_solver(level, starts, tol):
+        ws, st = [], []
+        for q, w in zip(level, starts):
+            w, s = O.lbfgs_wolfe(oprob(q), w, tol=tol)
+            err = O.max_rel_error(O.evaluate(oprob(q), w).mu, q.nu)
+            ws.append(w)
+            st.append(SimpleNamespace(iterations=s.iterations, max_rel_err=err, converged=s.converged))
+        return ws, st, 0.0
+
+    p = problems.make(2, 3, g=32, res=256)
+    ws, levels = multilevel.solve([p], min_sites=64, level_solver=level_solver)
+    assert [lv.n for lv in levels] == [64, 256, 1024]
+    assert [lv.tol for lv in levels] == [1e-3, 1e-3, 1e-4]
+    fine = levels[-1].stats[0]
+    assert fine.converged and fine.max_rel_err <= 1e-4
+    _, cold = O.lbfgs_wolfe(oprob(p), np.zeros(p.n), tol=1e-4)
+    assert fine.iterations < 0.8 * cold.iterations
