@@ -81,7 +81,8 @@ __global__ void __launch_bounds__(COT_NOALLOC_THREADS)
         const double g = mu[i] - nu[i];
         f += fc[i];
         const double rel = nu[i] > 0.0 ? fabs(g) / nu[i] : (g != 0.0 ? INFINITY : 0.0);
-        mx = fmax(mx, rel);
+        // a NaN mass must not look converged: fmax would drop it
+        mx = (rel == rel) ? fmax(mx, rel) : INFINITY;
         gn += g * g;
         emp += (mu[i] == 0.0) ? 1.0 : 0.0;
     }

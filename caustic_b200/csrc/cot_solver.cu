@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_eval(int n, const double
         f += fc[i] - wt[i] * nu[i];
         if (d != nullptr) gtd += g * d[i];
         double rel = nu[i] > 0.0 ? fabs(g) / nu[i] : (g != 0.0 ? INFINITY : 0.0);
-        mx = fmax(mx, rel);
+        mx = (rel == rel) ? fmax(mx, rel) : INFINITY;  // a NaN mass counts as unconverged
         gn += g * g;
         emp += (mu[i] == 0.0) ? 1.0 : 0.0;
         ovf += (nv[i] > max_ring) ? 1.0 : 0.0;

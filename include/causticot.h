@@ -273,7 +273,8 @@ COT_API int cot_render(cot_handle *h, const double *w, double gray_multiple, dou
  * allocations after start-up.  Reduces per-cell results already on the
  * device -- mu, f_cell, nu (n doubles each, device pointers, e.g. the outputs
  * of cot_eval with COT_MEM_DEVICE) -- to out[0..3] (device) =
- * {sum f_cell, max |mu - nu| / nu, sum (mu - nu)^2, count(mu == 0)}.
+ * {sum f_cell, max |mu - nu| / nu, sum (mu - nu)^2, count(mu == 0)};
+ * a NaN mass makes out[1] +inf, so that it never passes a tolerance.
  * Allocates nothing: its scratch is one fixed array per device
  * (COT_NOALLOC_MAX_BLOCKS x 4 doubles + a counter, about 32 KB) that every
  * GPU loading the library holds until exit; n above COT_NOALLOC_MAX_N is

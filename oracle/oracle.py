@@ -58,6 +58,7 @@ def lib():
             L = ctypes.CDLL(_LIB_PATH)
             L.orc_eval_cells.argtypes = [ctypes.c_int, _dp, _ip, _ip, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp]
             L.orc_clip_area.argtypes = [ctypes.c_int, _dp, _ip, _ip, _dp, _dp]
+            L.orc_edge_weights.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _ip, _ip, _dp, _dp, _ip, _dp, _dp]
             L.orc_center.argtypes = [ctypes.c_int, _dp, _ip, _ip, _dp, _ip, _dp, ctypes.c_int, _dp, _up]
             L.orc_render.argtypes = [ctypes.c_int, _dp, _ip, _ip, _dp, _ip, _dp, _dp]
             L.orc_cells.argtypes = [ctypes.c_int, _dp, _dp, _ip, _ip, _dp, ctypes.c_int, _ip, _dp, _ip]
@@ -202,6 +203,38 @@ def eval_cells(c: Cells, xy, w, nu, picture, size, proj_domain):
                      _d(_f64(nu)), _d(_f64(picture).reshape(-1)), _i(_i32(size)), _d(_f64(proj_domain)),
                      _d(mu), _d(f))
     return mu, f
+
+
+def edge_weights(c: Cells, xy, picture, size, proj_domain):
+    """a[i, k] = (integral of the density along ring edge k of cell i) /
+    (2 |s_i - s_j|) for an edge whose generator is a site j, else 0: the
+    off-diagonal entries -dmu_i/dw_j of the masses' Jacobian (no counterpart
+    in the reference; see orc_edge_weights)."""
+    L = lib()
+    n = c.ring_len.shape[0]
+    out = np.zeros((n, c.cap))
+    L.orc_edge_weights(n, c.cap, _d(_f64(c.ring_xy).reshape(-1)), _i(c.lens()), _i(_i32(c.ring_lab).reshape(-1)),
+                       _d(_f64(xy).reshape(-1)), _d(_f64(picture).reshape(-1)), _i(_i32(size)),
+                       _d(_f64(proj_domain)), _d(out.reshape(-1)))
+    return out
+
+
+def mass_jacobian(prob, w, c: Cells = None):
+    """Sparse dmu/dw at w (scipy CSR, n x n): a weighted graph Laplacian,
+    off-diagonal -a_ij from edge_weights, diagonal sum_j a_ij."""
+    import scipy.sparse as sp
+
+    if c is None:
+        c = cells(prob.xy, w, prob.box, prob.cap)
+    a = edge_weights(c, prob.xy, prob.picture, prob.size, prob.pd)
+    n = prob.n
+    lab = np.asarray(c.ring_lab)
+    rows = np.repeat(np.arange(n), c.cap).reshape(n, c.cap)
+    keep = (lab >= 0) & (a != 0.0)
+    r, j, v = rows[keep], lab[keep].astype(np.int64), a[keep]
+    H = sp.csr_matrix((-v, (r, j)), shape=(n, n))
+    H = H + sp.diags(a.sum(axis=1))
+    return H.tocsr()
 
 
 def clip_area(c: Cells, sample_domain):

@@ -472,3 +472,92 @@ ORC_API void orc_cells_brute(int n, const double *xy, const double *w, const dou
         free(all);
     }
 }
+
+/*
+ * Hessian of the masses (no counterpart in the reference, whose solvers use
+ * first derivatives only): for every ring edge k of cell i whose generator is
+ * a site j (lab >= 0),
+ *     a_k = (integral of rho along the edge) / (2 |s_i - s_j|) = -dmu_i/dw_j,
+ * and dmu_i/dw_i = sum_k a_k.  This is the classical derivative of a Laguerre
+ * cell's mass (Kitagawa, Merigot and Thibert, "Convergence of a Newton
+ * algorithm for semi-discrete optimal transport", J. Eur. Math. Soc. 2019,
+ * Thm 1.3): moving w_i by dw moves the edge towards j by dw / (2|s_i - s_j|).
+ * rho is the normalised picture per unit area (picture / pixel area); the
+ * edge is cut at every pixel line it crosses and each piece weighs the pixel
+ * that holds its midpoint.  Rings are fixed-stride (cap vertices per cell);
+ * out has the same layout (0 for domain sides and past the ring's end).
+ */
+static int orc_cmp_d(const void *a, const void *b)
+{
+    double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+
+static double orc_segment_rho(const double *P, const double *Q, const double *picture, const int *size,
+                              const double *pd, double xs, double ys)
+{
+    enum { TMAX = 16384 };
+    double ts[TMAX];
+    int nt = 0;
+    const double dx = Q[0] - P[0], dy = Q[1] - P[1];
+    const double len = sqrt(dx * dx + dy * dy);
+    if (!(len > 0)) return 0.0;
+    ts[nt++] = 0.0;
+    ts[nt++] = 1.0;
+    if (dx != 0.0) {
+        double a = (fmin(P[0], Q[0]) - pd[0]) / xs, b = (fmax(P[0], Q[0]) - pd[0]) / xs;
+        int c0 = (int)floor(a) + 1, c1 = (int)ceil(b) - 1;
+        if (c0 < 0) c0 = 0;
+        if (c1 > size[0]) c1 = size[0];
+        for (int c = c0; c <= c1; c++) {
+            if (nt >= TMAX) return NAN;  /* more crossings than the buffer holds: fail loudly */
+            double t = (pd[0] + c * xs - P[0]) / dx;
+            if (t > 0.0 && t < 1.0) ts[nt++] = t;
+        }
+    }
+    if (dy != 0.0) {
+        double a = (fmin(P[1], Q[1]) - pd[2]) / ys, b = (fmax(P[1], Q[1]) - pd[2]) / ys;
+        int r0 = (int)floor(a) + 1, r1 = (int)ceil(b) - 1;
+        if (r0 < 0) r0 = 0;
+        if (r1 > size[1]) r1 = size[1];
+        for (int r = r0; r <= r1; r++) {
+            if (nt >= TMAX) return NAN;
+            double t = (pd[2] + r * ys - P[1]) / dy;
+            if (t > 0.0 && t < 1.0) ts[nt++] = t;
+        }
+    }
+    qsort(ts, nt, sizeof(double), orc_cmp_d);
+    const double ga = xs * ys;
+    double acc = 0.0;
+    for (int k = 0; k + 1 < nt; k++) {
+        const double dt = ts[k + 1] - ts[k];
+        if (!(dt > 0)) continue;
+        const double tm = 0.5 * (ts[k] + ts[k + 1]);
+        const double mx = P[0] + tm * dx, my = P[1] + tm * dy;
+        const int ix = (int)floor((mx - pd[0]) / xs), iy = (int)floor((my - pd[2]) / ys);
+        if (ix < 0 || iy < 0 || ix >= size[0] || iy >= size[1]) continue;
+        acc += picture[ix + (size_t)iy * size[0]] / ga * dt;
+    }
+    return acc * len;
+}
+
+ORC_API void orc_edge_weights(int n, int cap, const double *ring, const int *len, const int *lab, const double *xy,
+                              const double *picture, const int *size, const double *pd, double *out)
+{
+    const double xs = (pd[1] - pd[0]) / (double)size[0];
+    const double ys = (pd[3] - pd[2]) / (double)size[1];
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n; i++) {
+        const double *R = ring + 2 * (size_t)i * cap;
+        double *o = out + (size_t)i * cap;
+        for (int k = 0; k < cap; k++) o[k] = 0.0;
+        const int m = len[i];
+        for (int k = 0; k < m; k++) {
+            const int j = lab[(size_t)i * cap + k];
+            if (j < 0) continue;
+            const double *P = R + 2 * k, *Q = R + 2 * ((k + 1) % m);
+            const double ex = xy[2 * j] - xy[2 * i], ey = xy[2 * j + 1] - xy[2 * i + 1];
+            o[k] = orc_segment_rho(P, Q, picture, size, pd, xs, ys) / (2.0 * sqrt(ex * ex + ey * ey));
+        }
+    }
+}

@@ -24,12 +24,11 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
 XIUSHI = "ustc_centerL_tri_standard_sp_parallel_light_rl"
 
 
-def main():
+def main(REF):
     pic = np.loadtxt(os.path.join(REF, "data/pic_data/ustc_centerL.txt"))
     assert np.all(pic == np.round(pic)) and pic.min() >= 0 and pic.max() <= 255
     np.savez_compressed(os.path.join(HERE, "ustc_centerL.npz"), picture=pic.astype(np.uint8))
@@ -74,4 +73,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of the reference repository checkout>")
+    main(sys.argv[1])

@@ -64,3 +64,23 @@ def test_noalloc_rejects_oversize_and_null(gpu):
     lib.cot_last_error(None, buf, 256)
     assert b"COT_NOALLOC_MAX_N" in buf.value
     assert lib.cot_eval_summary_noalloc(None, _ptr(a), _ptr(a), 8, _ptr(a), None) == capi.COT_EINVAL
+
+
+def test_noalloc_nan_mass_is_not_converged(gpu):
+    """A NaN among the masses must not vanish from the max-relative error
+    (a plain fmax would drop it and the summary would look converged)."""
+    import torch
+
+    lib = capi.load()
+    dev = torch.device("cuda", 0)
+    n = 5000
+    nu = torch.full((n,), 1.0 / n, dtype=torch.float64, device=dev)
+    mu = nu.clone()
+    mu[1234] = float("nan")
+    fc = torch.zeros(n, dtype=torch.float64, device=dev)
+    out = torch.zeros(4, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    assert lib.cot_eval_summary_noalloc(_ptr(mu), _ptr(fc), _ptr(nu), n, _ptr(out), None) == capi.COT_OK
+    torch.cuda.synchronize()
+    o = out.cpu().numpy()
+    assert o[1] == np.inf
