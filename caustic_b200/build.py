@@ -19,7 +19,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libcausticot.so")
 CLI = os.path.join(PKG, "caustic_GPU")
-CU_SOURCES = ["cot_cells.cu", "cot_solver.cu", "cot_capi.cu", "cot_noalloc.cu"]
+CU_SOURCES = ["cot_cells.cu", "cot_solver.cu", "cot_capi.cu", "cot_noalloc.cu", "cot_newton.cu"]
 WS_LIB = os.path.join(PKG, "libcausticws.so")
 WS_SOURCES = ["wsn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -41,7 +41,8 @@ def _stale(target, sources):
 
 def build_lib(force: bool = False, verbose: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES]
-    deps = srcs + [os.path.join(CSRC, "cot_common.cuh"), os.path.join(ROOT, "include", "causticot.h")]
+    deps = srcs + [os.path.join(CSRC, "cot_common.cuh"), os.path.join(CSRC, "cot_edge.cuh"),
+                   os.path.join(ROOT, "include", "causticot.h")]
     if not force and not _stale(LIB, deps):
         return LIB
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",

@@ -41,7 +41,7 @@ EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
     "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_source_masses_point_light", "cot_last_error",
-    "cot_set_progress", "cot_solve_batch",
+    "cot_set_progress", "cot_solve_batch", "cot_solve_newton", "cot_mass_jacobian",
 ]
 # int (*)(void *user, int phase, int iteration, int status, const double *w, const double *nu, int n,
 #         double grad_norm, double max_rel_err)
@@ -72,6 +72,33 @@ class cot_solve_stats(ctypes.Structure):
                 ("converged", ctypes.c_int), ("f", ctypes.c_double), ("max_rel_err", ctypes.c_double),
                 ("grad_norm", ctypes.c_double), ("empty_cells", ctypes.c_int),
                 ("ring_overflows", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
+class cot_newton_opts(ctypes.Structure):
+    _fields_ = [("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("cg_rtol", ctypes.c_double),
+                ("cg_max_iter", ctypes.c_int), ("lbfgs_chunk", ctypes.c_int), ("lbfgs_rounds", ctypes.c_int),
+                ("history", ctypes.c_int)]
+
+
+class cot_newton_stats(ctypes.Structure):
+    _fields_ = [("newton_iterations", ctypes.c_int), ("lbfgs_iterations", ctypes.c_int),
+                ("evaluations", ctypes.c_int), ("cg_iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("fallback", ctypes.c_int), ("max_rel_err", ctypes.c_double), ("grad_norm", ctypes.c_double),
+                ("empty_cells", ctypes.c_int), ("ms", ctypes.c_double)]
+
+
+@dataclass
+class NewtonStats:
+    newton_iterations: int
+    lbfgs_iterations: int
+    evaluations: int
+    cg_iterations: int
+    converged: bool
+    fallback: bool
+    max_rel_err: float
+    grad_norm: float
+    empty_cells: int
+    ms: float
 
 
 class cot_aarl_inputs(ctypes.Structure):
@@ -118,6 +145,9 @@ def load():
         L.cot_eval_summary_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         L.cot_solve_aarl.argtypes = [vp, vp, ctypes.POINTER(cot_aarl_inputs), ctypes.POINTER(cot_solve_opts),
                                      ctypes.POINTER(cot_solve_stats)]
+        L.cot_solve_newton.argtypes = [vp, vp, ctypes.POINTER(cot_newton_opts), ctypes.POINTER(cot_newton_stats),
+                                       ctypes.c_int]
+        L.cot_mass_jacobian.argtypes = [vp, vp, ctypes.c_int, ip, ip, dp, ctypes.c_int, ip]
         L.cot_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.cot_set_progress.argtypes = [vp, PROGRESS_FN, vp, ctypes.c_int]
         L.cot_solve_batch.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp),
@@ -317,6 +347,41 @@ class Solver:
         stats = SolveStats(st.iterations, st.evaluations, st.restarts, bool(st.converged), st.f, st.max_rel_err,
                            st.grad_norm, st.empty_cells, st.ring_overflows, st.ms)
         return w, stats
+
+    def solve_newton(self, w0, tol=1e-4, max_iter=100, cg_rtol=0.1, cg_max_iter=2000, lbfgs_chunk=10,
+                     lbfgs_rounds=50, history=10, raise_on_noconv=False):
+        """Damped Newton solve (cot_solve_newton): L-BFGS rounds while a cell
+        is empty, then Newton steps on the masses' Jacobian; L-BFGS finishes
+        if they stall.  Returns (weights, NewtonStats)."""
+        opts = cot_newton_opts(tol, max_iter, cg_rtol, cg_max_iter, lbfgs_chunk, lbfgs_rounds, history)
+        st = cot_newton_stats()
+        if _is_torch(w0):
+            w = w0.clone()
+            rc = self._L.cot_solve_newton(self._h, _tptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_DEVICE)
+        else:
+            w = _f64(w0).copy()
+            rc = self._L.cot_solve_newton(self._h, _vptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_HOST)
+        self._check(rc, allow=() if raise_on_noconv else (COT_ENOTCONV,))
+        return w, NewtonStats(st.newton_iterations, st.lbfgs_iterations, st.evaluations, st.cg_iterations,
+                              bool(st.converged), bool(st.fallback), st.max_rel_err, st.grad_norm, st.empty_cells,
+                              st.ms)
+
+    def mass_jacobian(self, w):
+        """dmu/dw at w as a scipy CSR matrix (cot_mass_jacobian)."""
+        import scipy.sparse as sp
+
+        w = _f64(w)
+        n = self.n
+        off = np.zeros(n + 1, dtype=np.int32)
+        nnz = ctypes.c_int(0)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self._check(self._L.cot_mass_jacobian(self._h, _vptr(w), COT_MEM_HOST, off.ctypes.data_as(ip), None, None,
+                                              0, ctypes.byref(nnz)))
+        cols = np.zeros(max(nnz.value, 1), dtype=np.int32)
+        vals = np.zeros(max(nnz.value, 1))
+        self._check(self._L.cot_mass_jacobian(self._h, _vptr(w), COT_MEM_HOST, off.ctypes.data_as(ip),
+                                              cols.ctypes.data_as(ip), _dptr(vals), cols.size, ctypes.byref(nnz)))
+        return sp.csr_matrix((vals[:nnz.value], cols[:nnz.value], off), shape=(n, n))
 
     def solve_aarl(self, w0, points, input_light, inside_light, height, *, z_of_len, z_of_receiver,
                    refraction_index, sample_domain, aa_history=7, aa_fixed_para=-2.0, lbfgs_prepass=True,

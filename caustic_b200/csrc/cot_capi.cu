@@ -22,6 +22,8 @@ struct CotProblemDev {
     int n = 0;
     int nb = 0;
     int nodes = 0;
+    size_t cap_n = 0, cap_nb = 0, cap_nodes = 0, cap_pix = 0;  // allocated sizes (grow only)
+    unsigned long long gen = 0;  // changes whenever the problem or its buffers change
     double2 *xy = nullptr;
     double *nu = nullptr;
     int *bstart = nullptr;
@@ -50,6 +52,17 @@ struct CotProblemDev {
     CotSolver *S = nullptr;
     double *Sv = nullptr, *Yv = nullptr;
     int hist_alloc = 0;
+    // Newton solve (allocated by its first call): the Jacobian rows (ELL,
+    // entry k of cell i at [k * n + i]), the rows of rings above 32
+    // vertices, the conjugate-gradient vectors and the step
+    double *hval = nullptr, *hdiag = nullptr, *hbig_val = nullptr;
+    int *hcol = nullptr, *hcnt = nullptr, *hbig_col = nullptr, *herr = nullptr;
+    int hbig_cap = 0;
+    double *nb_b = nullptr, *nb_r = nullptr, *nb_z = nullptr, *nb_pa = nullptr, *nb_pb = nullptr, *nb_q = nullptr;
+    double *nb_part = nullptr, *nb_tau = nullptr;
+    cot::PcgState *pcg = nullptr;
+    cot::NewtonEvalStats *nst = nullptr;
+    unsigned int *nticket = nullptr;
 };
 
 struct cot_handle {
@@ -62,6 +75,15 @@ struct cot_handle {
     CotProblemDev P;
     bool has_problem = false;
     CotSolver *hS = nullptr;  // pinned mirror of the control block
+    cot::NewtonEvalStats *hN = nullptr;  // pinned copies of the Newton solve's trial statistics
+    cot::PcgState *hP = nullptr;         // and of its inner solve's state
+    // the device-driven trial loop's graph, kept while the problem, its
+    // buffers and the stream stay the same (instantiating it costs more than
+    // a short solve of a small problem)
+    cudaGraphExec_t trial_exec = nullptr;
+    cudaStream_t trial_stream = nullptr;
+    unsigned long long trial_gen = 0;
+    long long trial_counts[3] = {0, 0, 0};
     cot::CotCtx ctx;
     // progress callback (cot_set_progress) and its caller-order buffers
     cot_progress_fn prog_fn = nullptr;
@@ -76,6 +98,7 @@ struct cot_handle {
 };
 
 static std::string g_create_err;
+static unsigned long long g_problem_gen = 0;  // problem generations (any handle)
 
 namespace cot {
 
@@ -138,7 +161,8 @@ static void free_problem(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
                     P.wq, P.fc, P.phibar, P.rbuf, P.lbuf, P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
-                    P.Yv};
+                    P.Yv, P.hval, P.hdiag, P.hbig_val, P.hcol, P.hcnt, P.hbig_col, P.herr, P.nb_b, P.nb_r, P.nb_z,
+                    P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.nb_tau, P.pcg, P.nst, P.nticket};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     P = CotProblemDev();
@@ -181,7 +205,11 @@ extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hS, sizeof(CotSolver));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hN, sizeof(NewtonEvalStats));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hP, sizeof(PcgState));
     if (e != cudaSuccess) {
+        if (h->hS) cudaFreeHost(h->hS);
+        if (h->hN) cudaFreeHost(h->hN);
         if (h->own_stream) cudaStreamDestroy(h->own_stream);
         delete h;
         return fail(nullptr, COT_ECUDA, "cot_create", cudaGetErrorString(e));
@@ -214,7 +242,10 @@ extern "C" int cot_destroy(cot_handle *h)
         for (int k = 0; k < h->ctx.ev_cap; k++) cudaEventDestroy(h->ctx.ev[k]);
         delete[] h->ctx.ev;
     }
+    if (h->trial_exec) cudaGraphExecDestroy(h->trial_exec);
     if (h->hS) cudaFreeHost(h->hS);
+    if (h->hN) cudaFreeHost(h->hN);
+    if (h->hP) cudaFreeHost(h->hP);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return COT_OK;
@@ -396,26 +427,41 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     std::vector<double> rho(dens.size());
     for (size_t p = 0; p < dens.size(); p++) rho[p] = (dens[p] / gray) / ga;
 
-    free_problem(P);
+    // buffers grow only: a problem that fits the current ones reuses them
+    // (the Newton buffers and the history included); a larger one
+    // reallocates everything at its own sizes
+    const bool fits = P.xy != nullptr && (size_t)n <= P.cap_n && (size_t)nb <= P.cap_nb &&
+                      (size_t)total <= P.cap_nodes && rho.size() <= P.cap_pix;
+    if (!fits) {
+        free_problem(P);
+        P.cap_n = (size_t)n;
+        P.cap_nb = (size_t)nb;
+        P.cap_nodes = (size_t)total;
+        P.cap_pix = rho.size();
+    }
     P.n = n;
     P.nb = nb;
     P.nodes = total;
     P.hperm = perm;
-    size_t N = (size_t)n;
-    auto A = [&](void **p, size_t bytes) -> cudaError_t { return cudaMalloc(p, bytes > 0 ? bytes : 16); };
+    P.gen = ++g_problem_gen;
+    const size_t N = P.cap_n;
+    auto A = [&](void **p, size_t bytes) -> cudaError_t {
+        if (*p != nullptr) return cudaSuccess;  // reused
+        return cudaMalloc(p, bytes > 0 ? bytes : 16);
+    };
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = A((void **)&P.xy, N * sizeof(double2));
     if (e == cudaSuccess) e = A((void **)&P.nu, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.bstart, (nb + 1) * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&P.bstart, (P.cap_nb + 1) * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.sbucket, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.tstat, total * sizeof(double4));
-    if (e == cudaSuccess) e = A((void **)&P.tdyn, total * sizeof(double4));
-    if (e == cudaSuccess) e = A((void **)&P.rho, rho.size() * 8);
+    if (e == cudaSuccess) e = A((void **)&P.tstat, P.cap_nodes * sizeof(double4));
+    if (e == cudaSuccess) e = A((void **)&P.tdyn, P.cap_nodes * sizeof(double4));
+    if (e == cudaSuccess) e = A((void **)&P.rho, P.cap_pix * 8);
     if (e == cudaSuccess) e = A((void **)&P.perm, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.w, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.wt, N * 8);
     if (e == cudaSuccess) e = A((void **)&P.wq, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.phibar, (size_t)nb * 8);
+    if (e == cudaSuccess) e = A((void **)&P.phibar, P.cap_nb * 8);
     if (e == cudaSuccess) e = A((void **)&P.rbuf, N * 32 * sizeof(double2));
     if (e == cudaSuccess) e = A((void **)&P.lbuf, N * 32 * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.cstate, N * sizeof(int));
@@ -431,7 +477,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
     if (e == cudaSuccess) e = A((void **)&P.nbn, N * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&P.nbn_q, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.partials, (size_t)reduce_blocks(n) * (5 * COT_MAX_HIST + 8) * 8);
+    if (e == cudaSuccess) e = A((void **)&P.partials, (size_t)reduce_blocks((int)P.cap_n) * (5 * COT_MAX_HIST + 8) * 8);
     if (e == cudaSuccess) e = A((void **)&P.ticket, sizeof(unsigned int));
     if (e == cudaSuccess) e = A((void **)&P.out, sizeof(CotEvalOut));
     if (e == cudaSuccess) e = A((void **)&P.tmp, 2 * N * 8);
@@ -440,17 +486,19 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
         free_problem(P);
         return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
     }
-    COT_CUDA_TRY(cudaMemcpyAsync(P.xy, sxy.data(), N * sizeof(double2), cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.nu, snu.data(), N * 8, cudaMemcpyHostToDevice, s));
+    const size_t Nn = (size_t)n;  // the copies move this problem's sizes, not the capacities
+    COT_CUDA_TRY(cudaMemcpyAsync(P.xy, sxy.data(), Nn * sizeof(double2), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.nu, snu.data(), Nn * 8, cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.bstart, cnt.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.sbucket, sb.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.sbucket, sb.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.tstat, tst.data(), total * sizeof(double4), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), N * sizeof(int), cudaMemcpyHostToDevice, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 16 * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, N * sizeof(int), s));
+    if (P.hcnt) COT_CUDA_TRY(cudaMemsetAsync(P.hcnt, 0, N * sizeof(int), s));
     COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
 
     CotGeo &g = P.geo;
@@ -943,10 +991,12 @@ static int solve_prepare(cot_handle *h, const cot_solve_opts &o)
         if (P.Yv) cudaFree(P.Yv);
         P.Sv = P.Yv = nullptr;
         P.hist_alloc = 0;
-        cudaError_t e = cudaMalloc(&P.Sv, (size_t)m * n * 8);
-        if (e == cudaSuccess) e = cudaMalloc(&P.Yv, (size_t)m * n * 8);
+        // sized for the buffers' capacity: a later problem that fits them reuses these
+        cudaError_t e = cudaMalloc(&P.Sv, (size_t)m * P.cap_n * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&P.Yv, (size_t)m * P.cap_n * 8);
         if (e != cudaSuccess) return fail(h, COT_ENOMEM, "solve: history allocation", cudaGetErrorString(e));
         P.hist_alloc = m;
+        P.gen = ++g_problem_gen;  // a graph that captured the old history buffers is stale
     }
     COT_CUDA_TRY(cudaMemsetAsync(P.Sv, 0, (size_t)m * n * 8, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.Yv, 0, (size_t)m * n * 8, s));
@@ -1025,7 +1075,26 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
     };
     cudaGraphExec_t exec = nullptr;
     BodyCounts bc;
-    if (o.use_graph >= 0 && build_trial_graph(h, tptr, &exec, &bc) == COT_OK) {
+    if (o.use_graph >= 0) {
+        if (h->trial_exec && h->trial_stream == s && h->trial_gen == P.gen) {
+            exec = h->trial_exec;
+            bc.launches = h->trial_counts[0];
+            bc.cell_launches = h->trial_counts[1];
+            bc.evaluations = h->trial_counts[2];
+        } else {
+            if (h->trial_exec) cudaGraphExecDestroy(h->trial_exec);
+            h->trial_exec = nullptr;
+            if (build_trial_graph(h, tptr, &exec, &bc) == COT_OK) {
+                h->trial_exec = exec;
+                h->trial_stream = s;
+                h->trial_gen = P.gen;
+                h->trial_counts[0] = bc.launches;
+                h->trial_counts[1] = bc.cell_launches;
+                h->trial_counts[2] = bc.evaluations;
+            }
+        }
+    }
+    if (exec != nullptr) {
         // device-driven loop: one graph launch runs trials until the solve is
         // done or the next progress report is due
         COT_CUDA_TRY(cudaMemcpyAsync(h->hS, P.S, ctl, cudaMemcpyDeviceToHost, s));
@@ -1055,7 +1124,6 @@ static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, 
         h->ctx.launches += bodies * bc.launches;
         h->ctx.cell_launches += bodies * bc.cell_launches;
         h->ctx.evaluations += bodies * bc.evaluations;
-        cudaGraphExecDestroy(exec);
         if (r != COT_OK) return stop(r);
     } else {
         // host-driven loop: one control-block read per trial
@@ -1564,4 +1632,322 @@ extern "C" int cot_solve_aarl(cot_handle *h, double *w_inout, const cot_aarl_inp
     }
     if (!converged) return failf(h, COT_ENOTCONV, "cot_solve_aarl: stopped after %d iterations (|g| %.3e)", iters, gnorm);
     return COT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// damped Newton solve and the masses' Jacobian (no counterpart in the
+// reference)
+// ---------------------------------------------------------------------------
+namespace cot {
+__global__ void k_rhs(int n, const double *__restrict__ nu, const double *__restrict__ mu, double *__restrict__ b)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = nu[i] - mu[i];
+}
+}  // namespace cot
+
+static int newton_alloc(cot_handle *h)
+{
+    CotProblemDev &P = h->P;
+    if (P.hval) return COT_OK;
+    // sized for the buffers' capacity: a later problem that fits them reuses these
+    const size_t N = P.cap_n;
+    const int pcg_blocks = pcg_max_blocks((int)N, h->num_sms);
+    P.hbig_cap = std::max(16, std::min((int)N, 4096));
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+    };
+    A((void **)&P.hval, 32 * N * sizeof(double));
+    A((void **)&P.hcol, 32 * N * sizeof(int));
+    A((void **)&P.hcnt, N * sizeof(int));
+    A((void **)&P.hdiag, N * sizeof(double));
+    A((void **)&P.hbig_val, (size_t)P.hbig_cap * COT_HBIG_W * sizeof(double));
+    A((void **)&P.hbig_col, (size_t)P.hbig_cap * COT_HBIG_W * sizeof(int));
+    A((void **)&P.herr, sizeof(int));
+    A((void **)&P.nb_b, N * 8);
+    A((void **)&P.nb_r, N * 8);
+    A((void **)&P.nb_z, N * 8);
+    A((void **)&P.nb_pa, N * 8);
+    A((void **)&P.nb_pb, N * 8);
+    A((void **)&P.nb_q, N * 8);
+    A((void **)&P.nb_part, (size_t)std::max(4 * pcg_blocks, 256 * 5) * 8);
+    A((void **)&P.nb_tau, 8);
+    A((void **)&P.pcg, sizeof(PcgState));
+    A((void **)&P.nst, sizeof(NewtonEvalStats));
+    A((void **)&P.nticket, sizeof(unsigned int));
+    if (e != cudaSuccess) {
+        void *ptrs[] = {P.hval, P.hcol, P.hcnt, P.hdiag, P.hbig_val, P.hbig_col, P.herr, P.nb_b, P.nb_r, P.nb_z,
+                        P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.nb_tau, P.pcg, P.nst, P.nticket};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        P.hval = P.hdiag = P.hbig_val = P.nb_b = P.nb_r = P.nb_z = P.nb_pa = P.nb_pb = P.nb_q = P.nb_part = P.nb_tau = nullptr;
+        P.hcol = P.hcnt = P.hbig_col = P.herr = nullptr;
+        P.pcg = nullptr;
+        P.nst = nullptr;
+        P.nticket = nullptr;
+        return fail(h, COT_ENOMEM, "cot_solve_newton: device allocation", cudaGetErrorString(e));
+    }
+    COT_CUDA_TRY(cudaMemsetAsync(P.nticket, 0, sizeof(unsigned int), h->stream));
+    COT_CUDA_TRY(cudaMemsetAsync(P.hcnt, 0, N * sizeof(int), h->stream));  // no row refers to a slot yet
+    return COT_OK;
+}
+
+// CellsArgs of an evaluation that keeps what the Jacobian needs: the final
+// rings' generators and the long rings' rows.
+static CellsArgs jacobian_args(CotProblemDev &P, const double *w, const double *d, const double *tptr)
+{
+    CellsArgs a = cells_args(P, w, d, tptr);
+    a.keep_labels = 1;
+    a.hbig_val = P.hbig_val;
+    a.hbig_col = P.hbig_col;
+    a.hbig_cap = P.hbig_cap;
+    a.hcnt = P.hcnt;
+    a.hdiag = P.hdiag;
+    a.herr = P.herr;
+    return a;
+}
+
+// One evaluation for the Newton solve at w + tau d (d == nullptr: at w),
+// then its statistics into *h->hN.
+static int newton_eval(cot_handle *h, const double *d)
+{
+    CotProblemDev &P = h->P;
+    CellsArgs a = jacobian_args(P, P.w, d, d ? P.nb_tau : nullptr);
+    COT_CUDA_TRY(cudaMemsetAsync(P.herr, 0, sizeof(int), h->stream));
+    launch_eval(P.geo, a, 1, h->num_sms, h->c());
+    launch_newton_stats(P.n, P.mut, P.nu, P.nv, P.nb_part, P.nticket, P.nst, h->c());
+    COT_CUDA_TRY(cudaGetLastError());
+    COT_CUDA_TRY(cudaMemcpyAsync(h->hN, P.nst, sizeof(NewtonEvalStats), cudaMemcpyDeviceToHost, h->stream));
+    COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return COT_OK;
+}
+
+extern "C" int cot_mass_jacobian(cot_handle *h, const double *w, int mem, int *row_offsets, int *cols, double *vals,
+                                 int capacity, int *nnz)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_mass_jacobian: no problem set", nullptr);
+    if (!w || !row_offsets || !nnz) return fail(h, COT_EINVAL, "cot_mass_jacobian: NULL argument", nullptr);
+    if (mem != COT_MEM_HOST && mem != COT_MEM_DEVICE) return fail(h, COT_EINVAL, "cot_mass_jacobian: bad mem flag", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    int r;
+    if ((r = newton_alloc(h)) != COT_OK) return r;
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    if ((r = upload_sorted(h, w, mem, P.wq)) != COT_OK) return r;
+    CellsArgs a = jacobian_args(P, P.wq, nullptr, nullptr);
+    COT_CUDA_TRY(cudaMemsetAsync(P.herr, 0, sizeof(int), s));
+    launch_eval(P.geo, a, 1, h->num_sms, h->c());
+    launch_hessian(P.geo, P.rbuf, P.lbuf, P.nv, P.hval, P.hcol, P.hcnt, P.hdiag, h->c());
+    COT_CUDA_TRY(cudaGetLastError());
+    const size_t N = (size_t)P.n;
+    std::vector<int> cnt(N), nv(N), hcol(32 * N);
+    std::vector<double> diag(N), hval(32 * N);
+    int herr = 0, nbig = 0;
+    COT_CUDA_TRY(cudaMemcpyAsync(cnt.data(), P.hcnt, N * sizeof(int), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(nv.data(), P.nv, N * sizeof(int), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(diag.data(), P.hdiag, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(hcol.data(), P.hcol, 32 * N * sizeof(int), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(hval.data(), P.hval, 32 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(&herr, P.herr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(&nbig, P.ovf_count + 7, sizeof(int), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < N; i++)
+        if (nv[i] > 256) return failf(h, COT_ERING, "cot_mass_jacobian: a cell has more than 256 vertices");
+    if (herr) return failf(h, COT_ECAPACITY, "cot_mass_jacobian: more than %d cells above 32 vertices", P.hbig_cap);
+    nbig = std::min(nbig, P.hbig_cap);
+    std::vector<int> bcol((size_t)nbig * COT_HBIG_W);
+    std::vector<double> bval((size_t)nbig * COT_HBIG_W);
+    if (nbig > 0) {
+        COT_CUDA_TRY(cudaMemcpyAsync(bcol.data(), P.hbig_col, bcol.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+        COT_CUDA_TRY(cudaMemcpyAsync(bval.data(), P.hbig_val, bval.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        COT_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    // rows in caller order, columns sorted, the diagonal included
+    std::vector<std::vector<std::pair<int, double>>> rows(N);
+    const std::vector<int> &perm = P.hperm;
+    for (size_t i = 0; i < N; i++) {
+        auto &row = rows[perm[i]];
+        row.emplace_back(perm[i], diag[i]);
+        if (cnt[i] >= 0) {
+            for (int k = 0; k < cnt[i]; k++) row.emplace_back(perm[hcol[k * N + i]], -hval[k * N + i]);
+        } else {
+            const size_t base = (size_t)(-cnt[i] - 1) * COT_HBIG_W;
+            if (base / COT_HBIG_W >= (size_t)nbig) return failf(h, COT_ECUDA, "cot_mass_jacobian: stale long-ring row");
+            for (int k = 0; k < COT_HBIG_W && bcol[base + k] >= 0; k++)
+                row.emplace_back(perm[bcol[base + k]], -bval[base + k]);
+        }
+        std::sort(row.begin(), row.end());
+    }
+    long long total = 0;
+    row_offsets[0] = 0;
+    for (size_t i = 0; i < N; i++) {
+        total += (long long)rows[i].size();
+        row_offsets[i + 1] = (int)std::min<long long>(total, INT_MAX);
+    }
+    *nnz = (int)std::min<long long>(total, INT_MAX);
+    if (!cols || !vals) return COT_OK;  // size query
+    if (total > capacity) return failf(h, COT_ECAPACITY, "cot_mass_jacobian: %lld entries, capacity %d", total, capacity);
+    size_t q = 0;
+    for (size_t i = 0; i < N; i++)
+        for (auto &e : rows[i]) {
+            cols[q] = e.first;
+            vals[q] = e.second;
+            q++;
+        }
+    return COT_OK;
+}
+
+extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton_opts *opts,
+                                cot_newton_stats *stats, int mem)
+{
+    if (!h) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_solve_newton: no problem set", nullptr);
+    if (!w_inout || !opts) return fail(h, COT_EINVAL, "cot_solve_newton: NULL argument", nullptr);
+    if (mem != COT_MEM_HOST && mem != COT_MEM_DEVICE) return fail(h, COT_EINVAL, "cot_solve_newton: bad mem flag", nullptr);
+    cot_newton_opts o = *opts;
+    if (!(o.tol > 0)) return fail(h, COT_EINVAL, "cot_solve_newton: tol must be positive", nullptr);
+    if (o.max_iter <= 0) o.max_iter = 100;
+    if (!(o.cg_rtol > 0) || o.cg_rtol >= 1.0) o.cg_rtol = 0.1;
+    if (o.cg_max_iter <= 0) o.cg_max_iter = 2000;
+    if (o.lbfgs_chunk <= 0) o.lbfgs_chunk = 10;
+    if (o.lbfgs_rounds <= 0) o.lbfgs_rounds = 50;
+    if (o.history <= 0) o.history = 10;
+    if (o.history > COT_MAX_HIST) return failf(h, COT_EINVAL, "cot_solve_newton: history must be in 1..%d", COT_MAX_HIST);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    int r;
+    if ((r = newton_alloc(h)) != COT_OK) return r;
+    CotProblemDev &P = h->P;
+    cudaStream_t s = h->stream;
+    cot_newton_stats st{};
+    if ((r = upload_sorted(h, w_inout, mem, P.w)) != COT_OK) return r;
+    cudaEvent_t e0, e1;
+    COT_CUDA_TRY(cudaEventCreate(&e0));
+    COT_CUDA_TRY(cudaEventCreate(&e1));
+    COT_CUDA_TRY(cudaEventRecord(e0, s));
+    auto finish = [&](int rc) -> int {
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        st.ms = t;
+        if (stats) *stats = st;
+        return rc;
+    };
+    // this library's L-BFGS, for the rounds with empty cells and the fall-back
+    cot_solve_opts lo{};
+    lo.mode = COT_SOLVE_WOLFE;
+    lo.history = o.history;
+    lo.tol = o.tol;
+    int rc = check_opts(h, lo);
+    if (rc != COT_OK) return finish(rc);
+    auto lbfgs = [&](int max_iter) -> int {
+        lo.max_iter = max_iter;
+        CotSolver hs;
+        const int rr = solve_device(h, lo, hs, nullptr, COT_PHASE_LBFGS, false);
+        if (rr != COT_OK) return rr;
+        st.lbfgs_iterations += hs.iter;
+        st.evaluations += hs.evals;
+        st.converged = hs.converged;
+        st.max_rel_err = hs.maxrel;
+        st.grad_norm = std::sqrt(hs.gnorm2);
+        st.empty_cells = hs.empty;
+        return COT_OK;
+    };
+    // 1. rounds of L-BFGS while some cell is empty (the Jacobian has no row
+    //    for an empty cell)
+    NewtonEvalStats cur{};
+    bool ready = false;
+    for (int round = 0; round <= o.lbfgs_rounds; round++) {
+        if ((rc = newton_eval(h, nullptr)) != COT_OK) return finish(rc);
+        st.evaluations++;
+        cur = *h->hN;
+        st.max_rel_err = cur.maxrel;
+        st.grad_norm = std::sqrt(cur.gnorm2);
+        st.empty_cells = cur.empty;
+        if (cur.maxrel <= o.tol) {
+            st.converged = 1;
+            break;
+        }
+        if (cur.empty == 0) {
+            ready = true;
+            break;
+        }
+        if (round == o.lbfgs_rounds) break;
+        if ((rc = lbfgs(o.lbfgs_chunk)) != COT_OK) return finish(rc);
+        if (st.converged) break;
+    }
+    // 2. damped Newton steps (Kitagawa, Merigot and Thibert 2019, Alg. 1):
+    //    solve dmu/dw d = nu - mu, then halve tau from 1 until every mass
+    //    stays above eps and |g(w + tau d)| <= (1 - tau / 2) |g(w)|
+    if (ready && !st.converged) {
+        double nu_min = INFINITY;
+        {
+            std::vector<double> hnu(P.n);
+            COT_CUDA_TRY(cudaMemcpyAsync(hnu.data(), P.nu, (size_t)P.n * 8, cudaMemcpyDeviceToHost, s));
+            COT_CUDA_TRY(cudaStreamSynchronize(s));
+            for (double v : hnu) nu_min = std::min(nu_min, v);
+        }
+        const double eps = 0.5 * std::min(nu_min, cur.minmu);
+        const int pcg_blocks = pcg_max_blocks(P.n, h->num_sms);
+        for (int it = 0; it < o.max_iter; it++) {
+            if (cur.maxrel <= o.tol) {
+                st.converged = 1;
+                break;
+            }
+            // the rings of the current point are the last evaluation's
+            int herr = 0;
+            COT_CUDA_TRY(cudaMemcpyAsync(&herr, P.herr, sizeof(int), cudaMemcpyDeviceToHost, s));
+            launch_hessian(P.geo, P.rbuf, P.lbuf, P.nv, P.hval, P.hcol, P.hcnt, P.hdiag, h->c());
+            k_rhs<<<nblk(P.n), 256, 0, s>>>(P.n, P.nu, P.mut, P.nb_b);
+            h->ctx.launches++;
+            PcgState zero{};
+            COT_CUDA_TRY(cudaMemcpyAsync(P.pcg, &zero, sizeof zero, cudaMemcpyHostToDevice, s));
+            COT_CUDA_TRY(launch_pcg(P.n, P.hval, P.hcol, P.hcnt, P.hbig_val, P.hbig_col, P.hdiag, P.nb_b, P.d, P.nb_r,
+                                    P.nb_z, P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.pcg, o.cg_rtol, o.cg_max_iter,
+                                    pcg_blocks, h->c()));
+            COT_CUDA_TRY(cudaMemcpyAsync(h->hP, P.pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+            COT_CUDA_TRY(cudaStreamSynchronize(s));
+            st.cg_iterations += h->hP->iterations;
+            if (herr != 0 || h->hP->error != 0) break;  // the fall-back below finishes
+            const double gn = std::sqrt(cur.gnorm2);
+            double tau = 1.0;
+            bool accepted = false;
+            for (int ls = 0; ls < 30; ls++) {
+                COT_CUDA_TRY(cudaMemcpyAsync(P.nb_tau, &tau, sizeof(double), cudaMemcpyHostToDevice, s));
+                if ((rc = newton_eval(h, P.d)) != COT_OK) return finish(rc);
+                st.evaluations++;
+                const NewtonEvalStats t = *h->hN;
+                if (t.minmu >= eps && std::sqrt(t.gnorm2) <= (1.0 - 0.5 * tau) * gn) {
+                    cur = t;
+                    accepted = true;
+                    break;
+                }
+                tau *= 0.5;
+            }
+            if (!accepted) break;  // the damped step stalled: the fall-back below finishes
+            // the accepted trial becomes the current point (its rings are in
+            // the buffers)
+            COT_CUDA_TRY(cudaMemcpyAsync(P.w, P.wt, (size_t)P.n * 8, cudaMemcpyDeviceToDevice, s));
+            st.newton_iterations++;
+            st.max_rel_err = cur.maxrel;
+            st.grad_norm = std::sqrt(cur.gnorm2);
+            st.empty_cells = cur.empty;
+        }
+        if (cur.maxrel <= o.tol) st.converged = 1;
+    }
+    // 3. fall-back: the L-BFGS from the last accepted point
+    if (!st.converged) {
+        st.fallback = 1;
+        if ((rc = lbfgs(INT_MAX / 2)) != COT_OK) return finish(rc);
+    }
+    if ((r = download_sorted(h, P.w, w_inout, mem)) != COT_OK) return finish(r);
+    COT_CUDA_TRY(cudaStreamSynchronize(s));
+    rc = finish(COT_OK);
+    if (!st.converged)
+        return failf(h, COT_ENOTCONV, "cot_solve_newton: stopped at max rel err %.3e", st.max_rel_err);
+    return rc;
 }

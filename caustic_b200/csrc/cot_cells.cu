@@ -22,6 +22,7 @@
 // plus the pixel's two vertical sides where they lie inside the cell.  Fully
 // covered pixels take a closed form.
 #include "cot_common.cuh"
+#include "cot_edge.cuh"
 #include <math.h>
 #include <algorithm>
 
@@ -1723,7 +1724,7 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
 
 // Phase 3: overflow hand-off, or the ring's integrals (EXACT) / the ring
 // buffer (solve path), the next evaluation's cache and the per-cell outputs.
-template <bool EXACT, int LPC>
+template <bool EXACT, int LPC, bool KEEP = false>
 __device__ __forceinline__ void cell_finish(const CotGeo &g, const CellsArgs &a, const int i, const double2 si,
                                             const double wi, RegPoly P, FastScratch &S, int *olist, int *ocount)
 {
@@ -1769,6 +1770,10 @@ __device__ __forceinline__ void cell_finish(const CotGeo &g, const CellsArgs &a,
             acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
         else if (lane < nv)
             a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.x, P.y);
+        // the Newton solve's Jacobian reads the final ring's generators
+        if constexpr (KEEP) {
+            if (lane < nv) a.lbuf[(size_t)i * COT_RCAP + lane] = P.l;
+        }
     }
     PSTAT_CLOCK(t3);
     PSTAT_ADD(2, t3 - t2);
@@ -1921,7 +1926,9 @@ __global__ void __launch_bounds__(128, MINB) k_cells_first(CotGeo g, CellsArgs a
     PSTAT_FLUSH();
 }
 
-template <int MINB>
+// KEEP: leave the final ring's generators in lbuf (the Newton solve's
+// Jacobian reads them); a separate instance keeps the solve's path as it is.
+template <int MINB, bool KEEP>
 __global__ void __launch_bounds__(128, MINB) k_cells_walk(CotGeo g, CellsArgs a)
 {
     constexpr int LPC = 32;
@@ -1959,7 +1966,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells_walk(CotGeo g, CellsArgs a)
         if (lane == 0) S.kn = -1;
         __syncwarp();
         P = cell_walk<LPC>(g, a, i, si, wi, P, (st & CST_CACHED) != 0, S);
-        cell_finish<false, LPC>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
+        cell_finish<false, LPC, KEEP>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
         __syncwarp();
     }
     PSTAT_FLUSH();
@@ -2226,6 +2233,56 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
             }
         }
         if (a.solid != nullptr && lane == 0) a.solid[i] = nv >= 3 ? solid_angle_of(P, nv, si, a.solid_z, a.solid_light) : 0.0;
+        if (a.keep_labels && nv >= 3) {
+            // the Newton solve's Jacobian: a ring that ended at most COT_RCAP
+            // vertices goes to the ring buffer like the fast path's rings, a
+            // longer one has its row built here
+            if (nv <= COT_RCAP) {
+                if (lane < nv) {
+                    a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.X[lane], P.Y[lane]);
+                    a.lbuf[(size_t)i * COT_RCAP + lane] = P.L[lane];
+                }
+            } else if (a.hbig_val != nullptr) {
+                int slot = 0;
+                if (lane == 0) slot = atomicAdd(a.ovf_count + 7, 1);
+                slot = __shfl_sync(FULLMASK, slot, 0);
+                if (slot >= a.hbig_cap) {
+                    if (lane == 0) atomicExch(a.herr, 1);
+                } else {
+                    const size_t base = (size_t)slot * COT_HBIG_W;
+                    int cnt = 0;
+                    double dsum = 0.0;
+                    for (int k0 = 0; k0 < nv; k0 += 32) {
+                        const int k = k0 + lane;
+                        double av = 0.0;
+                        int j = -1;
+                        if (k < nv) {
+                            j = P.L[k];
+                            if (j >= 0) {
+                                const int k1 = k + 1 == nv ? 0 : k + 1;
+                                const double2 sj = g.xy[j];
+                                const double ex = sj.x - si.x, ey = sj.y - si.y;
+                                av = edge_rho_integral(g, si.x + P.X[k], si.y + P.Y[k], si.x + P.X[k1], si.y + P.Y[k1]) /
+                                     (2.0 * sqrt(ex * ex + ey * ey));
+                            }
+                        }
+                        const unsigned site = __ballot_sync(FULLMASK, j >= 0);
+                        if (j >= 0) {
+                            const int pos = cnt + __popc(site & ((1u << lane) - 1u));
+                            a.hbig_val[base + pos] = av;
+                            a.hbig_col[base + pos] = j;
+                        }
+                        cnt += __popc(site);
+                        dsum += warp_sum(av);
+                    }
+                    if (lane == 0) {
+                        if (cnt < COT_HBIG_W) a.hbig_col[base + cnt] = -1;
+                        a.hcnt[i] = -(slot + 1);
+                        a.hdiag[i] = dsum;
+                    }
+                }
+            }
+        }
         if (a.nbn != nullptr) {
             // neighbours of this evaluation seed the next one
             int lab = -1;
@@ -2332,7 +2389,10 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
         const int bf = std::min(g.n, sms * (g_blocks_per_smf > 0 ? g_blocks_per_smf : FIRST_MINB) * CELLS_WPB);
         const size_t sm = sizeof(FastScratch) * CELLS_WPB;
         k_cells_first<FIRST_MINB><<<(bf + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
-        k_cells_walk<WALK_MINB><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+        if (a.keep_labels)
+            k_cells_walk<WALK_MINB, true><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+        else
+            k_cells_walk<WALK_MINB, false><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
         c.launches++;
     } else {
         launch_fast<false, 16>(g, a, 0, blocks, s);
@@ -2386,14 +2446,15 @@ void configure_cells_kernels()
         g_blocks_per_sm16 = nb;
     cudaFuncSetAttribute(k_integrate<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_first<FIRST_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
-    cudaFuncSetAttribute(k_cells_walk<WALK_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_cells_walk<WALK_MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_cells_walk<WALK_MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_first<FIRST_MINB>, 32 * CELLS_WPB, sm32) ==
             cudaSuccess &&
         nb > 0)
         g_blocks_per_smf = nb;
     nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_walk<WALK_MINB>, 32 * CELLS_WPB, sm32) ==
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_walk<WALK_MINB, false>, 32 * CELLS_WPB, sm32) ==
             cudaSuccess &&
         nb > 0)
         g_blocks_per_smw = nb;

@@ -153,7 +153,17 @@ struct CellsArgs {
     double *ring_xy;       // optional fixed-stride ring dump (nullable)
     int *ring_lab;
     int ring_cap;
+    // Newton solve only (zero elsewhere): the mass Jacobian's rows
+    int keep_labels;       // 1: the final ring's edge generators stay in lbuf
+    double *hbig_val;      // rows of rings above COT_RCAP vertices, COT_HBIG_W entries a slot (nullable)
+    int *hbig_col;
+    int hbig_cap;          // slots
+    int *hcnt;             // per cell: row length (ELL), or -(slot + 1) for a big row
+    double *hdiag;         // per cell: dmu_i/dw_i
+    int *herr;             // set when a big row found no slot
 };
+
+#define COT_HBIG_W 256  // entries of a big Jacobian row (the large-ring pass's capacity)
 
 void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms,
                  CotCtx &c);
@@ -174,6 +184,30 @@ void launch_loop_cond(cudaGraphConditionalHandle hc, const CotSolver *S, CotCtx 
 void launch_reject_cond(cudaGraphConditionalHandle hc, CotSolver *S, CotCtx &c);
 void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c);
 void configure_cells_kernels();
+
+// Launchers implemented in cot_newton.cu (the Newton solve's kernels).
+struct NewtonEvalStats {
+    double gnorm2;   // sum (mu - nu)^2
+    double minmu;    // min mu
+    double maxrel;   // max |mu - nu| / nu (+inf with a NaN)
+    int empty;       // cells with mu == 0
+    int maxnv;       // largest ring
+};
+struct PcgState {
+    int iterations;
+    int error;       // a grid barrier gave up waiting
+    double rr0, rr;  // squared residual norms at the start and the end
+    unsigned int bar_count, bar_gen;
+};
+void launch_hessian(const CotGeo &g, const double2 *rbuf, const int *lbuf, const int *nv, double *hval, int *hcol,
+                    int *hcnt, double *hdiag, CotCtx &c);
+void launch_newton_stats(int n, const double *mu, const double *nu, const int *nv, double *partials,
+                         unsigned int *ticket, NewtonEvalStats *out, CotCtx &c);
+int pcg_max_blocks(int n, int num_sms);
+cudaError_t launch_pcg(int n, const double *hval, const int *hcol, const int *hcnt, const double *hbig_val,
+                       const int *hbig_col, const double *hdiag, const double *b, double *x, double *r, double *z,
+                       double *pa, double *pb, double *q, double *partials, PcgState *st, double rtol, int max_it,
+                       int blocks, CotCtx &c);
 void launch_fcell_full(int n, const double *fc, const double *wt, const double *nu, double *out, CotCtx &c);
 void launch_fresnel_nu(int n, const double *cen, const double *src, const double *inl, const double *insl,
                        const double *hgt, const double *lam, double zl, double zr, double eta, double total,

@@ -28,8 +28,9 @@ from .problems import SDOTProblem
 def coarsen(p: SDOTProblem, min_pixels_per_site: int = 8) -> SDOTProblem:
     """The problem with each 2 x 2 block of sites merged (mean position,
     summed mass).  The image is merged 2 x 2 as well (pixel masses summed)
-    while it keeps at least ``min_pixels_per_site`` pixels across a coarse
-    site's pitch, so that a coarse evaluation costs less."""
+    when the unmerged image has at least ``min_pixels_per_site`` pixels
+    across a coarse site's pitch (so the merged image keeps at least half
+    that many), which makes a coarse evaluation cheaper."""
     gx, gy = p.grid
     if gx % 2 or gy % 2:
         raise ValueError(f"coarsen: site lattice {gx}x{gy} is not even")
@@ -82,8 +83,9 @@ class LevelStats:
     n: int                  # sites of the level
     image: tuple            # its image size
     tol: float              # the max-rel error it was solved to
-    stats: list = field(default_factory=list)   # SolveStats of each instance
+    stats: list = field(default_factory=list)   # SolveStats (NewtonStats) of each instance
     ms: float = 0.0         # device time of the level's (batched) solve
+    judge: list = field(default_factory=list)   # finest level: the plain L-BFGS's SolveStats per instance
 
 
 def _library_level(level, starts, tol, history, max_iter, batched):
@@ -108,21 +110,60 @@ def _library_level(level, starts, tol, history, max_iter, batched):
             s.close()
 
 
+def _newton_level(level, starts, tol, history, max_iter):
+    """One level with this library's damped Newton solve (cot_solve_newton),
+    instance by instance: (weights, NewtonStats list, device ms)."""
+    from . import capi
+
+    ws, sts = [], []
+    for q, w in zip(level, starts):
+        with capi.Solver() as s:
+            s.set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
+            wq, st = s.solve_newton(w, tol=tol, history=history)
+        ws.append(wq)
+        sts.append(st)
+    return ws, sts, float(sum(x.ms for x in sts))
+
+
+def _judge(probs, ws, tol, history):
+    """The plain L-BFGS (COT_SOLVE_WOLFE) from each result to ``tol``: it
+    evaluates the start and stops at once when the tolerance already holds,
+    else it finishes the solve.  Returns (weights, SolveStats list)."""
+    from . import capi
+
+    out, sts = [], []
+    for q, w in zip(probs, ws):
+        with capi.Solver() as s:
+            s.set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
+            wq, st = s.solve(w, mode=capi.SOLVE_WOLFE, tol=tol, history=history, max_iter=100000)
+        out.append(wq)
+        sts.append(st)
+    return out, sts
+
+
 def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float = 1e-3, min_sites: int = 1024,
           history: int = 10, max_iter: int = 100000, w0: Sequence[np.ndarray] = None, batched: bool = True,
-          level_solver=None):
+          level_solver=None, method: str = "lbfgs", judge: bool = False):
     """Solve every problem to max-rel error ``tol`` through its multilevel
     chain: the coarsest level from zero (or from ``w0``, one start vector
     per problem of the coarsest level's size), every other level from the
     level below, the coarse levels to ``coarse_tol``.  The problems' chains
-    are cut to the shortest one.  Each level runs as one batched solve
-    (cot_solve_batch) when ``batched``, else one solve per problem.
+    are cut to the shortest one.  With ``method="lbfgs"`` each level runs as
+    one batched solve (cot_solve_batch) when ``batched``, else one solve per
+    problem; with ``method="newton"`` each level is a damped Newton solve
+    (cot_solve_newton) per problem.  ``judge``: the plain L-BFGS then runs
+    from the finest level's weights to ``tol`` (it stops at its first
+    evaluation when the tolerance holds), so that the plain method decides
+    the error; its stats are the last level's ``judge``.
     Returns (weights of the finest level per problem, [LevelStats] from the
-    coarsest level up); a level's ``ms`` is its device time.
+    coarsest level up); a level's ``ms`` is its device time (the judge's
+    included).
 
     ``level_solver(problems, starts, tol)``, when given, solves a level in
     place of this library's solver and returns (weights, stats with
     ``iterations`` and ``max_rel_err``, ms)."""
+    if method not in ("lbfgs", "newton"):
+        raise ValueError(f"unknown method {method!r}")
     chains = [chain(p, min_sites) for p in probs]
     depth = min(len(c) for c in chains)
     chains = [c[:depth] for c in chains]
@@ -133,9 +174,15 @@ def solve(probs: Sequence[SDOTProblem], *, tol: float = 1e-4, coarse_tol: float 
         if k < depth - 1:
             ws = [prolong(w, c[k + 1], c[k]) for w, c in zip(ws, chains)]
         lt = tol if k == 0 else coarse_tol
-        if level_solver is None:
-            ws, st, ms = _library_level(level, ws, lt, history, max_iter, batched)
-        else:
+        if level_solver is not None:
             ws, st, ms = level_solver(level, ws, lt)
+        elif method == "newton":
+            ws, st, ms = _newton_level(level, ws, lt, history, max_iter)
+        else:
+            ws, st, ms = _library_level(level, ws, lt, history, max_iter, batched)
         levels.append(LevelStats(level[0].n, tuple(level[0].size), lt, list(st), ms))
+    if judge and level_solver is None:
+        ws, jst = _judge([c[0] for c in chains], ws, tol, history)
+        levels[-1].judge = jst
+        levels[-1].ms += float(sum(x.ms for x in jst))
     return ws, levels

@@ -178,6 +178,58 @@ COT_API int cot_solve(cot_handle *h, double *w_inout, const cot_solve_opts *opts
 COT_API int cot_solve_batch(cot_handle *const *handles, int count, double *const *w_inout,
                             const cot_solve_opts *opts, cot_solve_stats *stats);
 
+/* Options of the damped Newton solve (0 selects the default in brackets). */
+typedef struct {
+    double tol;          /* stop when max_i |mu_i - nu_i| / nu_i <= tol */
+    int max_iter;        /* Newton steps [100] */
+    double cg_rtol;      /* relative residual of each step's linear solve [0.1] */
+    int cg_max_iter;     /* conjugate-gradient iterations per step [2000] */
+    int lbfgs_chunk;     /* L-BFGS iterations per round while a cell is empty [10] */
+    int lbfgs_rounds;    /* such rounds before the Newton steps give up [50] */
+    int history;         /* L-BFGS memory of those rounds and of the fall-back [10] */
+} cot_newton_opts;
+
+typedef struct {
+    int newton_iterations;  /* accepted Newton steps */
+    int lbfgs_iterations;   /* L-BFGS iterations (empty-cell rounds and fall-back) */
+    int evaluations;        /* objective evaluations of both */
+    int cg_iterations;      /* conjugate-gradient iterations, summed over the steps */
+    int converged;
+    int fallback;           /* 1: the Newton steps stalled and the L-BFGS finished */
+    double max_rel_err;     /* at exit */
+    double grad_norm;       /* ||mu - nu||_2 at exit */
+    int empty_cells;
+    double ms;              /* device time */
+} cot_newton_stats;
+
+/* Damped Newton solve of the same problem to max_i |mu_i - nu_i| / nu_i <=
+ * tol.  No counterpart in the reference (its solvers are first-order:
+ * direct_ot's L-BFGS, ot_op.cuh:289-537, and aarl_direct_ot's Anderson
+ * acceleration).  The masses' Jacobian dmu/dw is a weighted graph Laplacian
+ * over the cells' shared edges: entry (i, j) is -(integral of the density
+ * along the edge) / (2 |s_i - s_j|).  Each step solves dmu/dw d = nu - mu by
+ * Jacobi-preconditioned conjugate gradients (one cooperative kernel) and
+ * halves the step until every mass stays above half its starting minimum and
+ * |mu - nu| falls by the factor (1 - tau/2) (Kitagawa, Merigot and Thibert,
+ * J. Eur. Math. Soc. 2019).  A cell that is empty has no row, so while some
+ * cell is empty the solve first runs rounds of this library's L-BFGS
+ * (COT_SOLVE_WOLFE, lbfgs_chunk iterations each); if the Newton steps stall
+ * the L-BFGS finishes from the last point (stats->fallback).  w_inout in
+ * caller order (mem: COT_MEM_HOST or COT_MEM_DEVICE).  COT_ENOTCONV when the
+ * tolerance was not reached. */
+COT_API int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton_opts *opts,
+                             cot_newton_stats *stats, int mem);
+
+/* The masses' Jacobian dmu/dw at weights w (caller order; w host or device
+ * per mem) as CSR in host memory: row i lists (j, dmu_i/dw_j) for j = i and
+ * every site j that shares an edge with cell i, columns ascending.
+ * row_offsets has n+1 entries; *nnz receives the entry count.  With cols or
+ * vals NULL only row_offsets and *nnz are filled (a size query); else
+ * capacity must be at least *nnz (COT_ECAPACITY).  No counterpart in the
+ * reference (the matrix of cot_solve_newton's steps). */
+COT_API int cot_mass_jacobian(cot_handle *h, const double *w, int mem, int *row_offsets, int *cols, double *vals,
+                              int capacity, int *nnz);
+
 /* Inputs of the Fresnel-reweighted solve (host arrays, caller order). */
 typedef struct {
     const double *points_xy;     /* source (lens) sites, 2n */

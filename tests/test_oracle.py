@@ -184,3 +184,30 @@ def test_green_integral_is_exact_second_moment():
     iy = ((5 - s[1]) ** 3 - (2 - s[1]) ** 3) / 3 * 2
     v = L.orc_poly_ints(O._d(sq), 4, O._d(s))
     assert abs(v - (ix + iy)) < 1e-12 * abs(ix + iy)
+
+
+def test_mass_jacobian_by_finite_differences():
+    """The masses' Jacobian (edge density integrals over 2|s_i - s_j|, the
+    Newton solve's matrix) against central differences of the masses."""
+    p = problems.make(1, g=12, res=48, beam=True)
+    prob = O.Problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+    rng = np.random.default_rng(4)
+    w = rng.normal(0, 0.3 / p.n, p.n)
+    J = O.mass_jacobian(prob, w)
+    assert abs(J - J.T).max() < 1e-12 * abs(J).max()           # symmetric
+    assert np.abs(np.asarray(J.sum(axis=1))).max() < 1e-12 * abs(J).max()   # rows sum to zero
+    for _ in range(3):
+        d = rng.normal(0, 1.0 / p.n, p.n)
+        eps = 1e-4
+        fd = (O.evaluate(prob, w + eps * d).mu - O.evaluate(prob, w - eps * d).mu) / (2 * eps)
+        assert np.abs(fd - J @ d).max() < 1e-5 * np.abs(fd).max()
+
+
+def test_mass_jacobian_known_answer():
+    """Two sites on a uniform density: the shared edge is the vertical line
+    x = 0.5 + (w0 - w1) of length 1, and |s0 - s1| = 0.5, so
+    dmu0/dw1 = -1 / (2 * 0.5) = -1."""
+    xy = np.array([[0.25, 0.5], [0.75, 0.5]])
+    prob = O.Problem(xy, np.array([0.5, 0.5]), np.full(16, 1 / 16.0), (4, 4), problems.UNIT_DOMAIN)
+    J = O.mass_jacobian(prob, np.array([0.05, 0.0])).toarray()
+    assert np.allclose(J, [[1.0, -1.0], [-1.0, 1.0]], atol=1e-14)

@@ -1,0 +1,35 @@
+"""Host logic of the warm-start pipeline (caustic_b200/warm.py), no GPU:
+which levels each start solves."""
+import pytest
+
+from caustic_b200 import problems
+from caustic_b200.warm import WarmSolver
+
+
+def test_levels_of_each_start():
+    p = problems.make(2, 0, g=128, res=512)          # 16,384 sites
+    ml = WarmSolver(start="multilevel")
+    assert [q.n for q in ml.chain(p)] == [16384, 4096, 1024]
+    z = WarmSolver(start="zero")
+    assert [q.n for q in z.chain(p)] == [16384]
+    learned = WarmSolver(start="learned", net=object(), net_level_sites=4096)
+    assert [q.n for q in learned.chain(p)] == [16384, 4096]
+    # a network for a level finer than the problem starts at the problem itself
+    fine = WarmSolver(start="learned", net=object(), net_level_sites=65536)
+    assert [q.n for q in fine.chain(p)] == [16384]
+
+
+def test_config2_learned_level_keeps_the_training_resolution():
+    """At the benchmark size the 16,384-site level has 4 pixels per site, as
+    the network's training problems do (128^2 sites, 512^2 images)."""
+    p = problems.make(2)
+    ch = WarmSolver(start="learned", net=object(), net_level_sites=16384).chain(p)
+    assert [q.n for q in ch] == [65536, 16384]
+    assert tuple(ch[-1].size) == (512, 512)
+
+
+def test_bad_arguments():
+    with pytest.raises(ValueError):
+        WarmSolver(start="sideways")
+    with pytest.raises(ValueError):
+        WarmSolver(start="learned")
