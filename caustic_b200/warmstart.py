@@ -17,7 +17,9 @@ Inputs (NHWC, 8 channels at the site grid's resolution, site grid G_x x G_y):
   0: log of the target density (pixels averaged onto the site grid),
      centred per image;
   1, 2: each site's jitter from its grid point, in quarter pitches;
-  3..7: zero (channel padding for the GEMM's 16-byte rows).
+  3: log(N * nu_i), each site's mass against the uniform 1/N (zero for
+     uniform masses, so a network trained on those alone sees no change);
+  4..7: zero (channel padding for the GEMM's 16-byte rows).
 Output: N * w / out_scale (weights scaled by the number of sites and by the
 spread of the training targets, stored with the network), compared with the
 solver's weights after removing each one's mean.
@@ -131,6 +133,9 @@ class WarmStartNet:
                 [] if c.b is None else [torch.zeros_like(c.b), torch.zeros_like(c.b)])
         self.step = 0
         self.out_scale = 1.0  # N * w = out_scale * output
+        # set to a list to record, per backward layer, (conv, dy, dz, dx): the
+        # incoming gradient, the bf16 gradient the GEMMs read and the result
+        self.trace = None
         self._ws = None
         self._ws_bytes = 0
 
@@ -218,9 +223,13 @@ class WarmStartNet:
         dcols = torch.empty(M, K, dtype=torch.float32, device=self.dev)
         self._gemm(GEMM_RR, M, K, c.cout, dz, c.w16, dcols)
         if c.k == 1:
+            if self.trace is not None:
+                self.trace.append((c, dy.clone(), dz.clone(), dcols.clone()))
             return dcols
         dx = torch.empty(M, c.cin, dtype=torch.float32, device=self.dev)
         _ok(L.ws_col2im(Bn, H, W, c.cin, _p(dcols), _p(dx), self._stream), "col2im")
+        if self.trace is not None:
+            self.trace.append((c, dy.clone(), dz.clone(), dx.clone()))
         return dx
 
     # -- network ----------------------------------------------------------
@@ -368,6 +377,7 @@ def make_input(probs, device="cuda"):
         x[..., 0] = lg
         x[..., 1] = jx
         x[..., 2] = jy
+        x[..., 3] = np.log(np.maximum(np.asarray(p.nu, np.float64) * p.n, 1e-300)).reshape(gy, gx)
         xs.append(x)
     return torch.from_numpy(np.stack(xs)).to(device=device, dtype=torch.bfloat16)
 
@@ -399,12 +409,23 @@ def predict(net: WarmStartNet, probs, batch: int = 32) -> list:
 # ---------------------------------------------------------------------------
 # data, training, evaluation
 # ---------------------------------------------------------------------------
-def solve_pairs(probs, tol: float = 1e-5, history: int = 10, chunk: int = 64):
-    """Converged weights of each problem (the training targets), solved from
-    w = 0 with batched solves (capi.solve_batch) to max-rel error tol."""
+def solve_pairs(probs, tol: float = 1e-5, history: int = 10, chunk: int = 64, method: str = "lbfgs"):
+    """Converged weights of each problem (the training targets) to max-rel
+    error tol: batched L-BFGS solves from w = 0 (capi.solve_batch), or with
+    method="newton" the multilevel damped Newton pipeline
+    (warm.WarmSolver), problem by problem."""
     from . import capi
 
     ws, stats = [], []
+    if method == "newton":
+        from .warm import WarmSolver
+
+        with WarmSolver(start="multilevel", tol=tol, min_sites=1024) as ws_:
+            for p in probs:
+                w, st = ws_.solve(p)
+                ws.append(w)
+                stats.append(st)
+        return ws, stats
     for k in range(0, len(probs), chunk):
         part = probs[k:k + chunk]
         sol = []
@@ -509,6 +530,12 @@ def main(argv=None) -> int:
     ap.add_argument("--base", type=int, default=32)
     ap.add_argument("--grid", type=int, default=0, help="sites per side (0: the configuration's 128)")
     ap.add_argument("--res", type=int, default=0, help="image pixels per side (0: the configuration's 256)")
+    ap.add_argument("--config", type=int, default=4,
+                    help="problem generator: 4 (uniform masses, K in 2..16) or 2 (beam masses, K = 16)")
+    ap.add_argument("--uniform-fraction", type=float, default=0.0,
+                    help="with --config 2: share of the pairs drawn with uniform masses instead of the beam")
+    ap.add_argument("--solver", choices=["lbfgs", "newton"], default="lbfgs",
+                    help="how the training targets are solved")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     kw = {}
@@ -517,9 +544,15 @@ def main(argv=None) -> int:
     if a.res:
         kw["res"] = a.res
     t0 = time.perf_counter()
-    train = [problems.make(4, i, **kw) for i in range(a.pairs)]
-    held = [problems.make(4, 100000 + i, **kw) for i in range(a.held)]
-    ws, st = solve_pairs(train, tol=1e-5)
+
+    def make(i):
+        if a.config == 2 and a.uniform_fraction > 0 and (i * 0.6180339887) % 1.0 < a.uniform_fraction:
+            return problems.make(2, i, beam=False, **kw)
+        return problems.make(a.config, i, **kw)
+
+    train = [make(i) for i in range(a.pairs)]
+    held = [make(100000 + i) for i in range(a.held)]
+    ws, st = solve_pairs(train, tol=1e-5, method=a.solver)
     t_data = time.perf_counter() - t0
     net = WarmStartNet(levels=a.levels, base=a.base, seed=0)
     X = make_input(train)

@@ -87,3 +87,62 @@ def test_training_and_warm_start_gain(gpu):
     # depend on the weights' differences at the pitch scale, which L-BFGS
     # still has to settle, so the saving is a fraction of the iterations
     assert np.mean(res["warm_iters"]) < 0.9 * np.mean(res["cold_iters"])
+
+
+def test_every_layer_matches_oracle_on_its_own_inputs(gpu):
+    """Layer by layer, on the GPU's own inputs to each layer (so BF16
+    rounding flips of earlier layers do not compound): forward
+    pre-activations, each weight and bias gradient, and each input gradient
+    agree with float64 sums of the same BF16 operands to 1e-5 (FP32
+    accumulation is the only difference), and the bf16 operands of the
+    backward GEMMs are bit-identical."""
+    import torch
+
+    rng = np.random.default_rng(8)
+    net = warmstart.WarmStartNet(levels=3, base=8, seed=5)
+    for c in net.layers():
+        if c.b is not None:
+            c.b.copy_(torch.from_numpy(rng.normal(0, 0.1, c.cout).astype(np.float32)))
+    x = R.bf16(rng.normal(size=(2, 16, 16, warmstart.IN_CH)))
+    t = rng.normal(size=(2, 256))
+    net.trace = []
+    pred = net.forward(bf16_tensor(torch, x), keep=True)
+    tape = [(c, cols.double().cpu().numpy(), None if pre is None else pre.double().cpu().numpy())
+            for (c, cols, pre, hh, ww) in net._tape[0]]
+    loss, g = net.loss_grad(pred, torch.from_numpy(t.astype(np.float32)).cuda())
+    net.zero_grad()
+    net.backward(g)
+    TOL = 1e-5
+
+    def rel(a, b):
+        return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+    for c, cols, pre in tape:
+        W = R.bf16(c.w.cpu().numpy().astype(np.float64))
+        d = cols @ W.T
+        if pre is not None:
+            assert rel(pre, d + c.b.cpu().numpy()) < TOL
+        else:
+            assert rel(pred.double().cpu().numpy().reshape(-1), d[:, 0]) < TOL
+    cols_of = {id(c): cols for c, cols, _ in tape}
+    pre_of = {id(c): pre for c, _, pre in tape}
+    assert len(net.trace) == len(tape)
+    for c, dy, dz, dx in net.trace:
+        dy = dy.double().cpu().numpy()
+        dz = dz.double().cpu().numpy()
+        pre = pre_of[id(c)]
+        if pre is not None:
+            # bias + ReLU backward, then the bf16 rounding of the GEMM operand
+            assert np.array_equal(dz, R.bf16(dy * (pre > 0)))
+            assert rel(c.gb.double().cpu().numpy(), (dy * (pre > 0)).sum(axis=0)) < TOL
+        else:
+            assert np.array_equal(dz, R.bf16(dy))
+        assert rel(c.gw.double().cpu().numpy(), dz.T @ cols_of[id(c)]) < TOL
+        dcols = dz @ R.bf16(c.w.cpu().numpy().astype(np.float64))
+        if c.k == 3:
+            M = dz.shape[0]
+            side = int(round(np.sqrt(M // 2)))
+            exp = R.col2im(dcols, (2, side, side, c.cin)).reshape(M, c.cin)
+        else:
+            exp = dcols
+        assert rel(dx.double().cpu().numpy(), exp) < TOL
