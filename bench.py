@@ -59,6 +59,10 @@ def parse():
                     help="cold against multilevel warm-started solves (config 2, 4 or 5)")
     ap.add_argument("--instances", type=int, default=0,
                     help="instances of a --multilevel run (0: 1 at config 2, 64 at config 4, 16 at config 5)")
+    ap.add_argument("--no-warm-start", action="store_true",
+                    help="skip the warm-started arms of the default run")
+    ap.add_argument("--warm-steps", type=int, default=0,
+                    help="timed solves of each warm-started arm (0: --steps)")
     return ap.parse_args()
 
 
@@ -192,6 +196,67 @@ def run_reference(args):
             "note": "the reference's own solver needs CGAL 5.5/Eigen/Boost, absent here; this is the oracle port"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+NET_C2 = os.path.join(ROOT, "caustic_b200", "data", "warmstart_c2.npz")
+NET_C2_LEVEL = 16384   # sites of the level the network predicts (128^2, 512^2 image at config 2)
+
+
+def warm_start_arms(args, p, cold_solve_ms, cold_e2e_ms, local):
+    """The metric's first half: warm-started solves of the same workload to
+    the same tolerance, each through warm.WarmSolver with the plain L-BFGS as
+    the judge at the end.  Every step is one whole solve from the host arrays
+    (coarsening, uploads, inference and the judge inside the timed region,
+    host wall clock with the device synchronised), compared with the cold
+    L-BFGS's device solve time (``value``'s solves) and its end-to-end time
+    (``e2e``'s solves)."""
+    import numpy as np
+    import torch
+
+    from caustic_b200.warm import WarmSolver
+
+    arms = {"multilevel": dict(start="multilevel")}
+    if os.path.exists(NET_C2):
+        from caustic_b200 import warmstart
+
+        net = warmstart.WarmStartNet.from_file(NET_C2, device=f"cuda:{local}")
+        arms["learned"] = dict(start="learned", net=net, net_level_sites=NET_C2_LEVEL)
+    out = {"cold_solve_ms": cold_solve_ms, "cold_e2e_ms": cold_e2e_ms,
+           "timing": "host wall clock per whole solve (host arrays in, weights out), device synchronised; "
+                     "device_ms sums the solves' CUDA-event times",
+           "learned": None if "learned" not in arms else {},
+           "learned_note": None if "learned" in arms else f"no trained network at {os.path.relpath(NET_C2, ROOT)}"}
+    steps = args.warm_steps or args.steps
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for name, kw in arms.items():
+        with WarmSolver(device=local, tol=args.tol, history=args.history, **kw) as ws:
+            for _ in range(args.warmup):
+                ws.solve(p)
+            walls, devs, infer, errs, conv, judge_it, levels = [], [], [], [], [], [], None
+            for k in range(steps):
+                flush.fill_(k & 255)
+                torch.cuda.synchronize()
+                w, st = ws.solve(p)
+                torch.cuda.synchronize()
+                walls.append(st.wall_ms)
+                devs.append(st.device_ms)
+                infer.append(st.infer_ms)
+                errs.append(st.max_rel_err)
+                conv.append(st.converged)
+                judge_it.append(st.judge.iterations)
+                levels = st.levels
+        wall = float(np.mean(walls))
+        dev = float(np.mean(devs))
+        out[name] = {"wall_ms": wall, "device_ms": dev, "infer_ms": float(np.mean(infer)),
+                     "speedup_wall_vs_cold_e2e": (cold_e2e_ms / wall) if cold_e2e_ms else None,
+                     "speedup_device_vs_cold": cold_solve_ms / dev,
+                     "max_rel_err": float(max(errs)), "converged": bool(all(conv)),
+                     "judge_iterations_max": int(max(judge_it)), "steps": steps,
+                     "levels": [{"n_sites": n, "newton_iterations": x.newton_iterations,
+                                 "lbfgs_iterations": x.lbfgs_iterations, "evaluations": x.evaluations,
+                                 "cg_iterations": x.cg_iterations, "fallback": x.fallback, "ms": x.ms}
+                                for n, x in levels]}
+    return out
 
 
 def run_ours(args):
@@ -349,6 +414,9 @@ def run_ours(args):
                 "max_rel_err": max(s.max_rel_err for s in stats), "converged": conv,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": ks["launches"]}
+        if world == 1 and not args.no_warm_start:
+            line["warm_start"] = warm_start_arms(args, p, tot_ms / args.steps,
+                                                 e2e["ms_per_step"] if e2e else None, local)
         print(json.dumps(line), flush=True)
     solver.close()
     if dist is not None:
