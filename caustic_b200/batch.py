@@ -19,7 +19,7 @@ import numpy as np
 
 from . import capi, problems
 
-CELLS_PER_WARP = (1, 2)
+CELLS_PER_WARP = (1, 2, 4)
 BUCKET_SIZES = (4, 8, 16)
 
 

@@ -185,9 +185,9 @@ extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
     if (cfg) h->cfg = *cfg;
     if (h->cfg.bucket_size <= 0) h->cfg.bucket_size = 16;
     if (h->cfg.cells_per_warp <= 0) h->cfg.cells_per_warp = 1;
-    if (h->cfg.cells_per_warp != 1 && h->cfg.cells_per_warp != 2) {
+    if (h->cfg.cells_per_warp != 1 && h->cfg.cells_per_warp != 2 && h->cfg.cells_per_warp != 4) {
         delete h;
-        return failf(nullptr, COT_EINVAL, "cot_create: cells_per_warp must be 1 or 2");
+        return failf(nullptr, COT_EINVAL, "cot_create: cells_per_warp must be 1, 2 or 4");
     }
     if (h->cfg.max_ring <= 0) h->cfg.max_ring = 200;
     h->device = h->cfg.device;

@@ -295,7 +295,7 @@ __device__ __forceinline__ double warp_max(double v)
 // within its own lanes only.
 template <int LPC>
 struct Seg {
-    static_assert(LPC == 32 || LPC == 16, "lanes per cell: 32 or 16");
+    static_assert(LPC == 32 || LPC == 16 || LPC == 8, "lanes per cell: 32, 16 or 8");
     static constexpr unsigned low = LPC == 32 ? FULLMASK : ((1u << (LPC & 31)) - 1u);
     unsigned mask;  // the segment's lanes in the warp
     int base;       // its first lane
@@ -1557,7 +1557,7 @@ __device__ __forceinline__ RegPoly cell_first(const CotGeo &g, const CellsArgs &
     if (cached) {
         const int lab = lane < ncache ? a.nbc[(size_t)i * COT_NBC + lane] : -1;
         bool direct = false;
-        if (nraw >= 3) {
+        if (nraw >= 3 && ncache <= LPC) {
             const double4 box = make_double4(g.pd[0] - si.x, g.pd[1] - si.x, g.pd[2] - si.y, g.pd[3] - si.y);
             const RegPoly Q = ring_from_cache<LPC>(lab, ncache, g.xy, box, si, wi, wt, lane, S);
             if (Q.nv != -2) {
@@ -1572,16 +1572,29 @@ __device__ __forceinline__ RegPoly cell_first(const CotGeo &g, const CellsArgs &
         if (!direct) {
             const int j = (lane < ncache && lab >= 0) ? lab : -1;
             P = apply_chunk_cold<LPC>(P, j, g.xy, si, wi, wt, lane, S, false);
+            if constexpr (LPC < COT_NBC) {
+                // the cached sites past the segment's lanes, a chunk at a time
+                for (int c0 = LPC; c0 < ncache && P.nv > 0; c0 += LPC) {
+                    const int lb = c0 + lane < ncache ? a.nbc[(size_t)i * COT_NBC + c0 + lane] : -1;
+                    P = apply_chunk_cold<LPC>(P, lb >= 0 ? lb : -1, g.xy, si, wi, wt, lane, S, false);
+                }
+            }
         }
         // a hidden cell that reappears gets the window as well, so that
         // the certificate starts from a tight ring
         if (hidden && P.nv > 0) cached = false;
     }
-    if (!cached && P.nv > 0) {
+    // the 3x3 buckets around the site: one round of lanes for 16 or 32, two
+    // for an 8-lane segment
+    constexpr int WROUNDS = LPC >= 16 ? 1 : 2;
+#pragma unroll
+    for (int r = 0; r < WROUNDS; r++) {
+        if (cached || P.nv <= 0) break;
+        const int k = r * LPC + lane;
         int bcnt = 0, bst = 0;
-        if (lane < 9) {
-            const int du = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
-            const int dv = (lane == 3 || lane == 5 || lane == 6) ? 1 : (lane == 4 || lane == 7 || lane == 8) ? -1 : 0;
+        if (k < 9) {
+            const int du = (k == 1 || k == 5 || k == 7) ? 1 : (k == 2 || k == 6 || k == 8) ? -1 : 0;
+            const int dv = (k == 3 || k == 5 || k == 6) ? 1 : (k == 4 || k == 7 || k == 8) ? -1 : 0;
             const int u = bu + du, v = bv + dv;
             if (u >= 0 && u < g.bx && v >= 0 && v < g.by) {
                 const int b = u + v * g.bx;
@@ -1622,8 +1635,10 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
         // start at the deepest level that still fits one round of lanes:
         // every node there is tested, a superset of what the levels above
         // would keep, without their rounds
+        // (at least the first level of at most 16 nodes: the levels above it
+        // are not built; an 8-lane segment takes it in two rounds)
         int top = g.nlev - 1;
-        while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= LPC) top--;
+        while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= (LPC < 16 ? 16 : LPC)) top--;
         int ncur = g.lev_w[top] * g.lev_h[top];
         if (ncur > COT_FRMAX) brute = true;
         int cur = 0;
@@ -2338,7 +2353,7 @@ static size_t cells_smem(int maxv, int warps)
 #ifndef WALK_MINB
 #define WALK_MINB 8   // k_cells_walk (64 registers; 6 blocks measured 2 % slower)
 #endif
-static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0, g_blocks_per_smi = 0;
+static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0, g_blocks_per_sm8 = 0, g_blocks_per_smi = 0;
 static int g_blocks_per_smf = 0, g_blocks_per_smw = 0;
 
 template <bool EXACT, int LPC>
@@ -2349,9 +2364,9 @@ static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int block
 }
 
 // One evaluation: bucket and tree bounds, then the cells.  cells_per_warp 2
-// runs the hot path on 16-lane segments (two cells per warp) with a 32-lane
-// second pass for rings above 16 vertices; every path ends with the
-// 256-vertex pass for rings above 32.
+// (4) runs the hot path on 16-lane (8-lane) segments, two (four) cells per
+// warp, with a 32-lane second pass for rings above 16 (8) vertices; every
+// path ends with the 256-vertex pass for rings above 32.
 void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms, CotCtx &c)
 {
     cudaStream_t s = c.s;
@@ -2374,12 +2389,13 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     }
     const int sms = num_sms > 0 ? num_sms : 148;
     const bool exact = a.cen != nullptr || a.splat != nullptr || a.solid != nullptr;
-    const int lpc = (exact || cells_per_warp < 2) ? 32 : 16;
+    const int lpc = (exact || cells_per_warp < 2) ? 32 : (cells_per_warp == 2 ? 16 : 8);
     const int per_sm32 = g_blocks_per_sm32 > 0 ? g_blocks_per_sm32 : CELLS_MINB;
     const int per_sm16 = g_blocks_per_sm16 > 0 ? g_blocks_per_sm16 : CELLS_MINB;
+    const int per_sm8 = g_blocks_per_sm8 > 0 ? g_blocks_per_sm8 : 1;
     const int cells_per_block = CELLS_WPB * (32 / lpc);
     const int want = (g.n + cells_per_block - 1) / cells_per_block;
-    const int blocks = std::min(want, sms * (lpc == 32 ? per_sm32 : per_sm16));
+    const int blocks = std::min(want, sms * (lpc == 32 ? per_sm32 : (lpc == 16 ? per_sm16 : per_sm8)));
     bool timed = c.profile && c.ev != nullptr && c.ev_used + 2 <= c.ev_cap;
     if (timed) cudaEventRecord(c.ev[c.ev_used], s);
     if (exact) {
@@ -2394,8 +2410,12 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
         else
             k_cells_walk<WALK_MINB, false><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
         c.launches++;
-    } else {
+    } else if (lpc == 16) {
         launch_fast<false, 16>(g, a, 0, blocks, s);
+        launch_fast<false, 32>(g, a, 1, sms, s);
+        c.launches++;
+    } else {
+        launch_fast<false, 8>(g, a, 0, blocks, s);
         launch_fast<false, 32>(g, a, 1, sms, s);
         c.launches++;
     }
@@ -2431,10 +2451,11 @@ extern "C" __attribute__((visibility("default"))) int cot_debug_phase_stats(unsi
 
 void configure_cells_kernels()
 {
-    const int sm32 = (int)(sizeof(FastScratch) * CELLS_WPB), sm16 = 2 * sm32;
+    const int sm32 = (int)(sizeof(FastScratch) * CELLS_WPB), sm16 = 2 * sm32, sm8 = 4 * sm32;
     cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm16);
+    cudaFuncSetAttribute(k_cells_fast<CELLS_MINB, false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm8);
     cudaFuncSetAttribute(k_cells<256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cells_smem(256, 1));
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false, 32>, 32 * CELLS_WPB,
@@ -2444,6 +2465,10 @@ void configure_cells_kernels()
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false, 16>, 32 * CELLS_WPB,
                                                       sm16) == cudaSuccess && nb > 0)
         g_blocks_per_sm16 = nb;
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_fast<CELLS_MINB, false, 8>, 32 * CELLS_WPB,
+                                                      sm8) == cudaSuccess && nb > 0)
+        g_blocks_per_sm8 = nb;
     cudaFuncSetAttribute(k_integrate<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_first<FIRST_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_walk<WALK_MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);

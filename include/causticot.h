@@ -75,8 +75,10 @@ typedef struct {
     int device;          /* CUDA device ordinal */
     int bucket_size;     /* target sites per neighbour bucket (0: default 16) */
     int cells_per_warp;  /* cells one warp works at once in the solve's cell
-                            kernel: 1 (32 lanes a cell) or 2 (16 lanes a cell,
-                            rings above 16 vertices redone on 32); 0: default */
+                            kernel: 1 (32 lanes a cell), 2 (16 lanes a cell,
+                            rings above 16 vertices redone on 32) or 4 (8
+                            lanes a cell, rings above 8 redone on 32); 0:
+                            default (1) */
     int max_ring;        /* ring-complexity reject threshold (0: 200, as
                             ot_op.cuh:376 max_edge_num/2) */
     int profile;         /* 1: time every cell-kernel launch with CUDA events

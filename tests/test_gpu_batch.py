@@ -58,7 +58,8 @@ def test_autotune_and_batched_config_instances(gpu):
     probs = batch.instances(6, res=64)
     assert len({p.n for p in probs}) > 3 and all(1024 * 0.9 <= p.n <= 32768 * 1.1 for p in probs)
     res = batch.autotune(probs, sample=3, max_iter=8, bucket_sizes=(8, 16))
-    assert len(res.table) == 4 and (res.cells_per_warp, res.bucket_size) in [(c, b) for c, b, _ in res.table]
+    assert len(res.table) == len(batch.CELLS_PER_WARP) * 2
+    assert (res.cells_per_warp, res.bucket_size) in [(c, b) for c, b, _ in res.table]
     ws, st, sec = batch.solve(probs[:3], cells_per_warp=res.cells_per_warp, bucket_size=res.bucket_size,
                               max_iter=40)
     assert sec > 0 and all(x.iterations <= 40 for x in st)
