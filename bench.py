@@ -84,17 +84,22 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """Per-launch DRAM bytes of the cell kernel from the committed ncu summary."""
+def committed_figure(key):
+    """A per-launch figure of the cell kernels from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "k_cells_config2.md")
     try:
         with open(path) as f:
             for line in f:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
+                if line.strip().startswith(key + ":"):
                     return float(line.split(":", 1)[1].strip().split()[0])
     except Exception:
         pass
     return None
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the cell kernels from the committed ncu summary."""
+    return committed_figure("traffic_bytes_per_launch")
 
 
 class Clocks:
@@ -414,6 +419,19 @@ def run_ours(args):
                 "max_rel_err": max(s.max_rel_err for s in stats), "converged": conv,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": ks["launches"]}
+        # the bound that does hold: warp-instruction issue (4 schedulers per
+        # SM, one warp instruction per cycle each, at the sampled SM clock)
+        insts = committed_figure("warp_instructions_per_launch")
+        ck = line["clocks"]
+        mhz = ck.get("sm_mhz") or ck.get("sm_max_mhz") or 1965.0
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        issue_peak = sms * 4 * mhz * 1e6
+        if insts and avg_ms > 0:
+            ach = insts / (avg_ms * 1e-3)
+            line["roofline_issue"] = {"bound": "issue", "achieved": ach, "peak": issue_peak, "unit": "warp-inst/s",
+                                      "frac": ach / issue_peak, "insts_per_launch": insts,
+                                      "peak_kind": f"{sms} SMs x 4 schedulers x 1 warp-inst/cycle at {mhz:.0f} MHz",
+                                      "insts_source": "smsp__inst_executed.sum, committed ncu summary"}
         if world == 1 and not args.no_warm_start:
             line["warm_start"] = warm_start_arms(args, p, tot_ms / args.steps,
                                                  e2e["ms_per_step"] if e2e else None, local)

@@ -21,7 +21,7 @@ LIB = os.path.join(PKG, "libcausticot.so")
 CLI = os.path.join(PKG, "caustic_GPU")
 CU_SOURCES = ["cot_cells.cu", "cot_solver.cu", "cot_capi.cu", "cot_noalloc.cu", "cot_newton.cu"]
 WS_LIB = os.path.join(PKG, "libcausticws.so")
-WS_SOURCES = ["wsn.cu"]
+WS_SOURCES = ["wsn.cu", "ws_predict.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

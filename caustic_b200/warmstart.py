@@ -164,6 +164,23 @@ class WarmStartNet:
             if c.b is not None:
                 c.b.copy_(torch.from_numpy(np.asarray(sd[f"b{k}"], np.float32)))
 
+    def save_bin(self, path: str):
+        """The flat binary that cot_warmstart_load (include/causticws.h) reads:
+        "CWS1", int32 levels, base, layer count, float64 out_scale, then per
+        layer (encoder, decoder, head) int32 cout, cin, k, has_bias and its
+        float32 weights [cout][k*k*cin] and biases [cout]."""
+        import struct
+
+        layers = list(self.layers())
+        with open(path, "wb") as f:
+            f.write(b"CWS1")
+            f.write(struct.pack("<iiid", self.levels, self.ch[0], len(layers), float(self.out_scale)))
+            for c in layers:
+                f.write(struct.pack("<iiii", c.cout, c.cin, c.k, 0 if c.b is None else 1))
+                f.write(np.ascontiguousarray(c.w.cpu().numpy(), np.float32).tobytes())
+                if c.b is not None:
+                    f.write(np.ascontiguousarray(c.b.cpu().numpy(), np.float32).tobytes())
+
     @classmethod
     def from_file(cls, path: str, device: str = "cuda"):
         sd = dict(np.load(path))
@@ -404,6 +421,58 @@ def predict(net: WarmStartNet, probs, batch: int = 32) -> list:
             w = row * net.out_scale / p.n
             out.append(w - w.mean())
     return out
+
+
+class CNet:
+    """The network through the C ABI (cot_warmstart_load / _predict, the
+    same entry points a C caller binds): load a file written by save_bin
+    once, then predict initial weights for problems on their site lattice."""
+
+    def __init__(self, path: str, device: int = 0):
+        L = load()
+        vp = ctypes.c_void_p
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.cot_warmstart_load.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]
+        L.cot_warmstart_free.argtypes = [vp]
+        L.cot_warmstart_predict.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int,
+                                            dp, dp, vp]
+        L.cot_warmstart_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        self._L = L
+        self._h = vp()
+        rc = L.cot_warmstart_load(path.encode(), device, ctypes.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"cot_warmstart_load: {rc}: {self.error()}")
+
+    def error(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        self._L.cot_warmstart_last_error(buf, 512)
+        return buf.value.decode()
+
+    def predict(self, p) -> np.ndarray:
+        dp = ctypes.POINTER(ctypes.c_double)
+        gx, gy = p.grid
+        xy = np.ascontiguousarray(p.xy, np.float64).reshape(-1)
+        nu = np.ascontiguousarray(p.nu, np.float64)
+        pic = np.ascontiguousarray(p.picture, np.float64)
+        pd = np.ascontiguousarray(p.proj_domain, np.float64)
+        out = np.zeros(p.n)
+        rc = self._L.cot_warmstart_predict(self._h, xy.ctypes.data_as(dp), nu.ctypes.data_as(dp), gx, gy,
+                                           pic.ctypes.data_as(dp), int(p.size[0]), int(p.size[1]),
+                                           pd.ctypes.data_as(dp), out.ctypes.data_as(dp), None)
+        if rc != 0:
+            raise RuntimeError(f"cot_warmstart_predict: {rc}: {self.error()}")
+        return out
+
+    def close(self):
+        if self._h:
+            self._L.cot_warmstart_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

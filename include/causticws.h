@@ -87,6 +87,30 @@ WS_API int ws_adam(long long n, float *w, void *w16, const float *g, float *m, f
                    float b2, float eps, int step, void *stream);
 WS_API int ws_to_bf16(long long n, const float *x, void *y, void *stream);
 
+/* ---- the learned warm start as one call (no counterpart in the reference:
+ * its solver starts from the previous outer iteration's weights or zero,
+ * main.cu:193-198) ------------------------------------------------------- */
+typedef struct ws_net ws_net;
+
+/* Load a network saved by WarmStartNet.save_bin (caustic_b200/warmstart.py)
+ * onto `device`: BF16 weights and FP32 biases stay there until
+ * cot_warmstart_free. */
+WS_API int cot_warmstart_load(const char *path, int device, ws_net **out);
+WS_API int cot_warmstart_free(ws_net *net);
+
+/* Initial dual weights for the problem of a gx x gy jittered site lattice
+ * (sites_xy[2*(a + gx*b)], caller order, inside proj_domain), target masses
+ * nu[n] and density image density[ix + iy*nx] (any positive scale; nx and ny
+ * whole multiples of gx and gy, gx and gy multiples of 2^(levels-1)): the
+ * network's prediction with its mean removed, into w_out[n] (host memory;
+ * all inputs are host arrays too).  The plain solve (cot_solve) then starts
+ * from w_out; the inputs are prepared as warmstart.make_input does. */
+WS_API int cot_warmstart_predict(ws_net *net, const double *sites_xy, const double *nu, int gx, int gy,
+                                 const double *density, int nx, int ny, const double proj_domain[4], double *w_out,
+                                 void *stream);
+/* Message of the last failure of the three calls above. */
+WS_API int cot_warmstart_last_error(char *buf, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -146,3 +146,26 @@ def test_every_layer_matches_oracle_on_its_own_inputs(gpu):
         else:
             exp = dcols
         assert rel(dx.double().cpu().numpy(), exp) < TOL
+
+
+def test_c_abi_predict_matches_python(gpu, tmp_path):
+    """cot_warmstart_predict (a C caller's learned start) gives the Python
+    host layer's prediction: same inputs, same kernels, same weights."""
+    import torch
+
+    rng = np.random.default_rng(12)
+    net = warmstart.WarmStartNet(levels=3, base=8, seed=9)
+    for c in net.layers():
+        if c.b is not None:
+            c.b.copy_(torch.from_numpy(rng.normal(0, 0.1, c.cout).astype(np.float32)))
+    net.out_scale = 3.7
+    path = str(tmp_path / "net.bin")
+    net.save_bin(path)
+    cn = warmstart.CNet(path)
+    for p in (problems.make(2, 3, g=16, res=64), problems.make(4, 5, g=32, res=64)):
+        ref = warmstart.predict(net, [p])[0]
+        got = cn.predict(p)
+        assert np.abs(got - ref).max() <= 1e-3 * np.abs(ref).max()
+    with pytest.raises(RuntimeError):
+        cn.predict(problems.make(4, 5, g=10, res=40))   # 10 is not a multiple of 2^(levels-1) = 4
+    cn.close()

@@ -56,7 +56,7 @@ def test_bf16_rounding_is_nearest_even():
 def test_kernel_library_exports_its_header():
     build.build_ws()
     with open(os.path.join(ROOT, "include", "causticws.h")) as f:
-        names = re.findall(r"WS_API\s+\w+\s+(ws_\w+)\s*\(", f.read())
+        names = re.findall(r"WS_API\s+\w+\s+((?:ws|cot_warmstart)_\w+)\s*\(", f.read())
     assert "ws_gemm" in names and "ws_adam" in names
     lib = ctypes.CDLL(warmstart.WS_LIB)
     assert not [n for n in names if not hasattr(lib, n)]
