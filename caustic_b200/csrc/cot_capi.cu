@@ -980,7 +980,7 @@ static int build_trial_graph(cot_handle *h, double *tptr, cudaGraphExec_t *exec,
 
 // History buffers and the device control block of a solve from the weights
 // in P.w, on the handle's stream.
-static int solve_prepare(cot_handle *h, const cot_solve_opts &o)
+static int solve_prepare(cot_handle *h, const cot_solve_opts &o, int stop_nonempty = 0)
 {
     CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
@@ -1015,19 +1015,20 @@ static int solve_prepare(cot_handle *h, const cot_solve_opts &o)
     hs.f = INFINITY;
     hs.need_begin = 1;
     hs.pause_iter = INT_MAX;
+    hs.stop_nonempty = stop_nonempty;
     if (o.max_iter == 0) hs.done = 1;
     COT_CUDA_TRY(cudaMemcpyAsync(P.S, &hs, sizeof(CotSolver), cudaMemcpyHostToDevice, s));
     return COT_OK;
 }
 
 static int solve_device(cot_handle *h, const cot_solve_opts &o, CotSolver &out, float *ms, int phase,
-                        bool report_start)
+                        bool report_start, int stop_nonempty = 0)
 {
     CotProblemDev &P = h->P;
     cudaStream_t s = h->stream;
     CotSolver &hs = *h->hS;
     int rp;
-    if ((rp = solve_prepare(h, o)) != COT_OK) return rp;
+    if ((rp = solve_prepare(h, o, stop_nonempty)) != COT_OK) return rp;
     cudaEvent_t e0, e1;
     COT_CUDA_TRY(cudaEventCreate(&e0));
     COT_CUDA_TRY(cudaEventCreate(&e1));
@@ -1844,10 +1845,10 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
     lo.tol = o.tol;
     int rc = check_opts(h, lo);
     if (rc != COT_OK) return finish(rc);
-    auto lbfgs = [&](int max_iter) -> int {
+    auto lbfgs = [&](int max_iter, int stop_nonempty) -> int {
         lo.max_iter = max_iter;
         CotSolver hs;
-        const int rr = solve_device(h, lo, hs, nullptr, COT_PHASE_LBFGS, false);
+        const int rr = solve_device(h, lo, hs, nullptr, COT_PHASE_LBFGS, false, stop_nonempty);
         if (rr != COT_OK) return rr;
         st.lbfgs_iterations += hs.iter;
         st.evaluations += hs.evals;
@@ -1857,8 +1858,10 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
         st.empty_cells = hs.empty;
         return COT_OK;
     };
-    // 1. rounds of L-BFGS while some cell is empty (the Jacobian has no row
-    //    for an empty cell)
+    // 1. L-BFGS while some cell is empty (the Jacobian has no row for an
+    //    empty cell): one run that stops as soon as every cell has mass, at
+    //    most lbfgs_chunk x lbfgs_rounds iterations (a run that ends early,
+    //    e.g. a failed line search, is started again)
     NewtonEvalStats cur{};
     bool ready = false;
     for (int round = 0; round <= o.lbfgs_rounds; round++) {
@@ -1876,8 +1879,9 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
             ready = true;
             break;
         }
-        if (round == o.lbfgs_rounds) break;
-        if ((rc = lbfgs(o.lbfgs_chunk)) != COT_OK) return finish(rc);
+        const int left = o.lbfgs_chunk * o.lbfgs_rounds - st.lbfgs_iterations;
+        if (round == o.lbfgs_rounds || left <= 0) break;
+        if ((rc = lbfgs(left, 1)) != COT_OK) return finish(rc);
         if (st.converged) break;
     }
     // 2. damped Newton steps (Kitagawa, Merigot and Thibert 2019, Alg. 1):
@@ -1942,7 +1946,7 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
     // 3. fall-back: the L-BFGS from the last accepted point
     if (!st.converged) {
         st.fallback = 1;
-        if ((rc = lbfgs(INT_MAX / 2)) != COT_OK) return finish(rc);
+        if ((rc = lbfgs(INT_MAX / 2, 0)) != COT_OK) return finish(rc);
     }
     if ((r = download_sorted(h, P.w, w_inout, mem)) != COT_OK) return finish(r);
     COT_CUDA_TRY(cudaStreamSynchronize(s));

@@ -80,7 +80,7 @@ struct CotSolver {
     int max_ls;
     int max_iter;
     int max_ring;
-    int opt_pad;
+    int stop_nonempty;   // 1: the solve also stops (unconverged) once no cell is empty
     double c1, c2, t0, tol;
     double H0;
     double rho[COT_MAX_HIST];

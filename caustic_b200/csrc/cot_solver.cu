@@ -488,7 +488,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
     S->maxrel = S->last.maxrel;
     S->gnorm2 = S->last.gnorm2;
     S->empty = S->last.empty;
-    if (initial) return;
+    if (initial) {
+        // a Wolfe-mode solve whose start already meets the tolerance stops at
+        // its first evaluation (as the oracle's restatement does); the
+        // reference mode always takes an iteration, as direct_ot does
+        if (S->mode == COT_SOLVE_WOLFE && S->maxrel <= S->tol) {
+            S->converged = 1;
+            S->done = 1;
+        }
+        if (S->stop_nonempty && S->empty == 0) S->done = 1;
+        return;
+    }
     double ys = G[(m + h) * COT_BASIS + h];
     double yy = G[(m + h) * COT_BASIS + (m + h)];
     if (S->mode == COT_SOLVE_REFERENCE) {
@@ -508,6 +518,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_accept(int n, CotSolver *S, dou
     } else {
         if (S->maxrel <= S->tol) { S->converged = 1; S->done = 1; }
     }
+    if (S->stop_nonempty && S->empty == 0) S->done = 1;
     if (S->iter >= S->max_iter) S->done = 1;
 }
 

@@ -66,6 +66,21 @@ def prolong(wc: np.ndarray, coarse: SDOTProblem, fine: SDOTProblem) -> np.ndarra
     return w - w.mean()
 
 
+def restrict(wf: np.ndarray, fine: SDOTProblem, coarse: SDOTProblem) -> np.ndarray:
+    """Weights of ``fine`` averaged over the blocks of sites that make up
+    each site of ``coarse`` (a lattice coarser by a power of two per side,
+    as ``chain`` builds it), with their mean removed.  A coarse site is the
+    mean of its block, and w is smooth in the site position, so the block
+    mean is the weight at the coarse site up to the lattice's curvature."""
+    gxf, gyf = fine.grid
+    gxc, gyc = coarse.grid
+    if gxf % gxc or gyf % gyc:
+        raise ValueError("restrict: the coarse lattice does not divide the fine one")
+    fx, fy = gxf // gxc, gyf // gyc
+    w = np.asarray(wf, np.float64).reshape(gyc, fy, gxc, fx).mean(axis=(1, 3)).ravel()
+    return w - w.mean()
+
+
 def chain(p: SDOTProblem, min_sites: int = 1024, max_levels: int = 8) -> list:
     """[p, coarser, ...]: halve the lattice while both sides stay even and
     the next level keeps at least ``min_sites`` sites."""

@@ -186,8 +186,9 @@ typedef struct {
     int max_iter;        /* Newton steps [100] */
     double cg_rtol;      /* relative residual of each step's linear solve [0.1] */
     int cg_max_iter;     /* conjugate-gradient iterations per step [2000] */
-    int lbfgs_chunk;     /* L-BFGS iterations per round while a cell is empty [10] */
-    int lbfgs_rounds;    /* such rounds before the Newton steps give up [50] */
+    int lbfgs_chunk;     /* while a cell is empty the L-BFGS runs, stopping as */
+    int lbfgs_rounds;    /* soon as none is, for at most lbfgs_chunk x
+                            lbfgs_rounds iterations [10 x 50] */
     int history;         /* L-BFGS memory of those rounds and of the fall-back [10] */
 } cot_newton_opts;
 
@@ -214,8 +215,8 @@ typedef struct {
  * halves the step until every mass stays above half its starting minimum and
  * |mu - nu| falls by the factor (1 - tau/2) (Kitagawa, Merigot and Thibert,
  * J. Eur. Math. Soc. 2019).  A cell that is empty has no row, so while some
- * cell is empty the solve first runs rounds of this library's L-BFGS
- * (COT_SOLVE_WOLFE, lbfgs_chunk iterations each); if the Newton steps stall
+ * cell is empty the solve first runs this library's L-BFGS
+ * (COT_SOLVE_WOLFE) until every cell has mass; if the Newton steps stall
  * the L-BFGS finishes from the last point (stats->fallback).  w_inout in
  * caller order (mem: COT_MEM_HOST or COT_MEM_DEVICE).  COT_ENOTCONV when the
  * tolerance was not reached. */

@@ -184,6 +184,22 @@ def test_wolfe_solve_matches_oracle(gpu):
     assert O.max_rel_error(O.evaluate(oracle_problem(p), w).mu, p.nu) <= 1e-4
 
 
+def test_wolfe_solve_from_a_converged_start_stops_at_once(gpu):
+    """The plain L-BFGS as the judge of a warm start: from weights that meet
+    the tolerance it evaluates once and takes no iteration (the oracle's
+    lbfgs_wolfe checks the start the same way), in both loops."""
+    p = problems.make(1, g=16, res=64)
+    s = solver_for(p)
+    w, st = s.solve(np.zeros(p.n), mode=capi.SOLVE_WOLFE, tol=1e-6, history=10)
+    assert st.converged
+    for use_graph in (0, -1):
+        w2, st2 = s.solve(w, mode=capi.SOLVE_WOLFE, tol=1e-4, history=10, use_graph=use_graph)
+        assert st2.converged and st2.iterations == 0 and st2.evaluations == 1
+        assert np.array_equal(w2, w)
+    _, ost = O.lbfgs_wolfe(oracle_problem(p), w, tol=1e-4, m=10)
+    assert ost.converged and ost.iterations == 0 and ost.evaluations == 1
+
+
 def test_wolfe_solve_passes_the_evaluation_noise_floor(gpu):
     """The device line search tolerates the objective's evaluation noise as
     the oracle does (approximate Wolfe): a small problem solves to 1e-10."""
