@@ -77,7 +77,7 @@ class cot_solve_stats(ctypes.Structure):
 class cot_newton_opts(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("cg_rtol", ctypes.c_double),
                 ("cg_max_iter", ctypes.c_int), ("lbfgs_chunk", ctypes.c_int), ("lbfgs_rounds", ctypes.c_int),
-                ("history", ctypes.c_int)]
+                ("history", ctypes.c_int), ("shrink_steps", ctypes.c_int)]
 
 
 class cot_newton_stats(ctypes.Structure):
@@ -349,11 +349,13 @@ class Solver:
         return w, stats
 
     def solve_newton(self, w0, tol=1e-4, max_iter=100, cg_rtol=0.1, cg_max_iter=2000, lbfgs_chunk=10,
-                     lbfgs_rounds=50, history=10, raise_on_noconv=False):
-        """Damped Newton solve (cot_solve_newton): L-BFGS rounds while a cell
+                     lbfgs_rounds=50, history=10, shrink_steps=0, raise_on_noconv=False):
+        """Damped Newton solve (cot_solve_newton): optionally a scaled-down
+        start when the start empties cells (shrink_steps), L-BFGS while a cell
         is empty, then Newton steps on the masses' Jacobian; L-BFGS finishes
         if they stall.  Returns (weights, NewtonStats)."""
-        opts = cot_newton_opts(tol, max_iter, cg_rtol, cg_max_iter, lbfgs_chunk, lbfgs_rounds, history)
+        opts = cot_newton_opts(tol, max_iter, cg_rtol, cg_max_iter, lbfgs_chunk, lbfgs_rounds, history,
+                               shrink_steps)
         st = cot_newton_stats()
         if _is_torch(w0):
             w = w0.clone()

@@ -1816,6 +1816,7 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
     if (o.lbfgs_rounds <= 0) o.lbfgs_rounds = 50;
     if (o.history <= 0) o.history = 10;
     if (o.history > COT_MAX_HIST) return failf(h, COT_EINVAL, "cot_solve_newton: history must be in 1..%d", COT_MAX_HIST);
+    o.shrink_steps = std::min(std::max(o.shrink_steps, 0), 30);
     COT_CUDA_TRY(cudaSetDevice(h->device));
     int r;
     if ((r = newton_alloc(h)) != COT_OK) return r;
@@ -1864,6 +1865,28 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
     //    e.g. a failed line search, is started again)
     NewtonEvalStats cur{};
     bool ready = false;
+    if (o.shrink_steps > 0) {
+        // the start scaled towards w = 0 (a power diagram at w = 0 is the
+        // Voronoi diagram, which empties no cell inside the density's
+        // support): the largest of 1/2, 1/4, ... that empties none.  The
+        // trial weights w + tau w with tau = s - 1 are exactly s w.
+        if ((rc = newton_eval(h, nullptr)) != COT_OK) return finish(rc);
+        st.evaluations++;
+        if (h->hN->empty > 0 && h->hN->maxrel > o.tol) {
+            double sc = 1.0;
+            for (int k = 0; k < o.shrink_steps; k++) {
+                sc *= 0.5;
+                double tau = sc - 1.0;
+                COT_CUDA_TRY(cudaMemcpyAsync(P.nb_tau, &tau, sizeof(double), cudaMemcpyHostToDevice, s));
+                if ((rc = newton_eval(h, P.w)) != COT_OK) return finish(rc);
+                st.evaluations++;
+                if (h->hN->empty == 0) {
+                    COT_CUDA_TRY(cudaMemcpyAsync(P.w, P.wt, (size_t)P.n * 8, cudaMemcpyDeviceToDevice, s));
+                    break;
+                }
+            }
+        }
+    }
     for (int round = 0; round <= o.lbfgs_rounds; round++) {
         if ((rc = newton_eval(h, nullptr)) != COT_OK) return finish(rc);
         st.evaluations++;

@@ -25,6 +25,13 @@ import numpy as np
 from .problems import SDOTProblem
 
 
+def _sum2x2(a: np.ndarray) -> np.ndarray:
+    """Sums of the 2 x 2 blocks of the first two axes, (a00 + a01) + (a10 +
+    a11), by strided adds (several times faster than a reshaped axis sum)."""
+    r = a[:, 0::2] + a[:, 1::2]
+    return r[0::2] + r[1::2]
+
+
 def coarsen(p: SDOTProblem, min_pixels_per_site: int = 8) -> SDOTProblem:
     """The problem with each 2 x 2 block of sites merged (mean position,
     summed mass).  The image is merged 2 x 2 as well (pixel masses summed)
@@ -34,12 +41,12 @@ def coarsen(p: SDOTProblem, min_pixels_per_site: int = 8) -> SDOTProblem:
     gx, gy = p.grid
     if gx % 2 or gy % 2:
         raise ValueError(f"coarsen: site lattice {gx}x{gy} is not even")
-    xy = p.xy.reshape(gy // 2, 2, gx // 2, 2, 2).mean(axis=(1, 3)).reshape(-1, 2)
-    nu = p.nu.reshape(gy // 2, 2, gx // 2, 2).sum(axis=(1, 3)).ravel()
+    xy = 0.25 * _sum2x2(np.asarray(p.xy, np.float64).reshape(gy, gx, 2)).reshape(-1, 2)
+    nu = _sum2x2(np.asarray(p.nu, np.float64).reshape(gy, gx)).ravel()
     W, H = p.size
     pic, size = p.picture, p.size
     if W % 2 == 0 and H % 2 == 0 and W // (gx // 2) >= min_pixels_per_site and H // (gy // 2) >= min_pixels_per_site:
-        pic = np.asarray(p.picture, np.float64).reshape(H // 2, 2, W // 2, 2).sum(axis=(1, 3)).ravel()
+        pic = _sum2x2(np.asarray(p.picture, np.float64).reshape(H, W)).ravel()
         size = (W // 2, H // 2)
     return SDOTProblem(p.name + "/coarse", xy, nu, pic, size, np.array(p.proj_domain, np.float64), (gx // 2, gy // 2))
 
@@ -50,19 +57,23 @@ def prolong(wc: np.ndarray, coarse: SDOTProblem, fine: SDOTProblem) -> np.ndarra
     (b + 0.5) / G_y) of the domain; held constant beyond the outer sites),
     with their mean removed."""
     gxc, gyc = coarse.grid
-    Wc = np.asarray(wc, np.float64).reshape(gyc, gxc)
+    Wc = np.asarray(wc, np.float64).ravel()
     d = np.asarray(fine.proj_domain, np.float64)
-    ux = (fine.xy[:, 0] - d[0]) / (d[1] - d[0])
-    uy = (fine.xy[:, 1] - d[2]) / (d[3] - d[2])
-    x = np.clip(ux * gxc - 0.5, 0.0, gxc - 1.0)
-    y = np.clip(uy * gyc - 0.5, 0.0, gyc - 1.0)
-    x0 = np.minimum(np.floor(x).astype(np.int64), max(gxc - 2, 0))
-    y0 = np.minimum(np.floor(y).astype(np.int64), max(gyc - 2, 0))
-    x1 = np.minimum(x0 + 1, gxc - 1)
-    y1 = np.minimum(y0 + 1, gyc - 1)
-    fx, fy = x - x0, y - y0
-    w = (Wc[y0, x0] * (1 - fx) * (1 - fy) + Wc[y0, x1] * fx * (1 - fy) + Wc[y1, x0] * (1 - fx) * fy
-         + Wc[y1, x1] * fx * fy)
+    x = (fine.xy[:, 0] - d[0]) * (gxc / (d[1] - d[0])) - 0.5
+    y = (fine.xy[:, 1] - d[2]) * (gyc / (d[3] - d[2])) - 0.5
+    np.clip(x, 0.0, gxc - 1.0, out=x)
+    np.clip(y, 0.0, gyc - 1.0, out=y)
+    x0 = np.minimum(x.astype(np.int64), max(gxc - 2, 0))   # x >= 0: truncation is the floor
+    y0 = np.minimum(y.astype(np.int64), max(gyc - 2, 0))
+    fx = x - x0
+    fy = y - y0
+    i00 = x0 + y0 * gxc
+    dx = 1 if gxc > 1 else 0
+    dy = gxc if gyc > 1 else 0
+    w00, w01, w10, w11 = Wc[i00], Wc[i00 + dx], Wc[i00 + dy], Wc[i00 + dx + dy]
+    a = w00 + fx * (w01 - w00)
+    b = w10 + fx * (w11 - w10)
+    w = a + fy * (b - a)
     return w - w.mean()
 
 

@@ -50,7 +50,7 @@ class WarmStats:
 class WarmSolver:
     def __init__(self, start: str = "multilevel", net=None, net_level_sites: int = 0, min_sites: int = 1024,
                  tol: float = 1e-4, coarse_tol: float = 1e-3, history: int = 10, device: int = 0,
-                 learned_at: str = "coarsest"):
+                 learned_at: str = "coarsest", shrink_steps: int = 0):
         if start not in ("multilevel", "learned", "zero"):
             raise ValueError(f"unknown start {start!r}")
         if start == "learned" and net is None:
@@ -58,6 +58,7 @@ class WarmSolver:
         if learned_at not in ("coarsest", "level"):
             raise ValueError(f"unknown learned_at {learned_at!r}")
         self.learned_at = learned_at
+        self.shrink_steps = shrink_steps
         self.start = start
         self.net = net
         self.net_level_sites = net_level_sites
@@ -129,7 +130,8 @@ class WarmSolver:
                 w = multilevel.prolong(w, ch[k + 1], q)
             s = self._handle(k)
             s.set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
-            w, st = s.solve_newton(w, tol=self.tol if k == 0 else self.coarse_tol, history=self.history)
+            w, st = s.solve_newton(w, tol=self.tol if k == 0 else self.coarse_tol, history=self.history,
+                                   shrink_steps=self.shrink_steps)
             levels.append((q.n, st))
             lwall.append(1e3 * (time.perf_counter() - tl))
             dev_ms += st.ms

@@ -190,6 +190,10 @@ typedef struct {
     int lbfgs_rounds;    /* soon as none is, for at most lbfgs_chunk x
                             lbfgs_rounds iterations [10 x 50] */
     int history;         /* L-BFGS memory of those rounds and of the fall-back [10] */
+    int shrink_steps;    /* when the start leaves a cell empty: try the start
+                            scaled by 1/2, 1/4, ... (this many times) and keep
+                            the first that empties none, before any L-BFGS;
+                            the weights w = 0 never empty a cell [0: off] */
 } cot_newton_opts;
 
 typedef struct {
