@@ -63,6 +63,8 @@ def parse():
                     help="skip the warm-started arms of the default run")
     ap.add_argument("--warm-steps", type=int, default=0,
                     help="timed solves of each warm-started arm (0: --steps)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched configuration's sub-object of the default run")
     return ap.parse_args()
 
 
@@ -264,6 +266,53 @@ def warm_start_arms(args, p, cold_solve_ms, cold_e2e_ms, local):
     return out
 
 
+def batched_arms(args, local, stream):
+    """The batched configuration beside the headline: its 64 seeded instances
+    (N log-uniform in [1,024, 32,768], 512^2 targets) solved to the same
+    tolerance (i) by the plain L-BFGS in one graph launch after the
+    autotuner picked the cell kernel's shape (cells per warp {1, 2, 4} x
+    sites per bucket {4, 8, 16}), (ii) one after another (the sequential
+    pass), and (iii) by the warm-start pipeline instance by instance (host
+    arrays in, weights out, host wall clock).  One run of each."""
+    import numpy as np
+    import torch
+
+    from caustic_b200 import batch
+    from caustic_b200.warm import WarmSolver
+
+    probs = batch.instances(64)
+    opts = dict(tol=args.tol, history=args.history, max_iter=100000)
+    tune = batch.autotune(probs, stream=stream.cuda_stream, tol=args.tol, history=args.history)
+    kw = dict(cells_per_warp=tune.cells_per_warp, bucket_size=tune.bucket_size, stream=stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    batch.solve(probs[:8], **kw, **opts)          # warm-up
+    flush.fill_(1)
+    torch.cuda.synchronize()
+    _, st, sec = batch.solve(probs, **kw, **opts)
+    flush.fill_(2)
+    torch.cuda.synchronize()
+    _, sq, sq_sec = batch.solve_sequential(probs, **kw, **opts)
+    with WarmSolver(device=local, tol=args.tol, history=args.history) as ws:
+        ws.solve(probs[0])                          # warm-up
+        flush.fill_(3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        wst = [ws.solve(p)[1] for p in probs]
+        torch.cuda.synchronize()
+        warm_sec = time.perf_counter() - t0
+    return {"instances": 64, "n_range": [min(p.n for p in probs), max(p.n for p in probs)], "image": [512, 512],
+            "batched_solves_per_s": 64 / sec, "batched_converged": all(x.converged for x in st),
+            "batched_max_rel_err": max(x.max_rel_err for x in st),
+            "batched_cell_evals_per_s": sum(p.n * x.evaluations for p, x in zip(probs, st)) / sec,
+            "sequential_solves_per_s": 64 / sq_sec, "batched_over_sequential": sq_sec / sec,
+            "warm_pipeline_solves_per_s": 64 / warm_sec, "warm_over_batched": sec / warm_sec,
+            "warm_converged": all(x.converged for x in wst), "warm_max_rel_err": max(x.max_rel_err for x in wst),
+            "timing": "batched and sequential: device time of the solves; warm: host wall clock of the 64 pipelines",
+            "autotune": {"cells_per_warp": tune.cells_per_warp, "bucket_size": tune.bucket_size,
+                         "table": [{"cells_per_warp": c, "bucket_size": b, "cell_evals_per_s": r}
+                                   for c, b, r in tune.table]}}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -435,6 +484,8 @@ def run_ours(args):
         if world == 1 and not args.no_warm_start:
             line["warm_start"] = warm_start_arms(args, p, tot_ms / args.steps,
                                                  e2e["ms_per_step"] if e2e else None, local)
+        if world == 1 and not args.no_batched:
+            line["batched_config3"] = batched_arms(args, local, stream)
         print(json.dumps(line), flush=True)
     solver.close()
     if dist is not None:
