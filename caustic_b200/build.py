@@ -19,7 +19,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libcausticot.so")
 CLI = os.path.join(PKG, "caustic_GPU")
-CU_SOURCES = ["cot_cells.cu", "cot_solver.cu", "cot_capi.cu", "cot_noalloc.cu", "cot_newton.cu"]
+CU_SOURCES = ["cot_cells.cu", "cot_solver.cu", "cot_capi.cu", "cot_noalloc.cu", "cot_newton.cu", "cot_build.cu"]
 WS_LIB = os.path.join(PKG, "libcausticws.so")
 WS_SOURCES = ["wsn.cu", "ws_predict.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

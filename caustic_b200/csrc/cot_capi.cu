@@ -23,6 +23,13 @@ struct CotProblemDev {
     int nb = 0;
     int nodes = 0;
     size_t cap_n = 0, cap_nb = 0, cap_nodes = 0, cap_pix = 0;  // allocated sizes (grow only)
+    // set-up scratch: partial sums, their tickets, the input statistics,
+    // the sort's temporary storage
+    double *bpart = nullptr;
+    unsigned int *bticket = nullptr;
+    unsigned char *bstat = nullptr;
+    void *cubtmp = nullptr;
+    size_t cubtmp_bytes = 0;
     unsigned long long gen = 0;  // changes whenever the problem or its buffers change
     double2 *xy = nullptr;
     double *nu = nullptr;
@@ -77,6 +84,7 @@ struct cot_handle {
     CotSolver *hS = nullptr;  // pinned mirror of the control block
     cot::NewtonEvalStats *hN = nullptr;  // pinned copies of the Newton solve's trial statistics
     cot::PcgState *hP = nullptr;         // and of its inner solve's state
+    unsigned char *hB = nullptr;         // pinned copy of the set-up's input statistics
     // the device-driven trial loop's graph, kept while the problem, its
     // buffers and the stream stay the same (instantiating it costs more than
     // a short solve of a small problem)
@@ -157,14 +165,44 @@ static inline int nblk(int n) { return (n + 255) / 256; }
 
 using namespace cot;
 
-static void free_problem(CotProblemDev &P)
+// The buffers sized by the sites and pixels (with the Newton buffers and
+// the L-BFGS history, which are sized by the sites too).
+static void free_sized_by_sites(CotProblemDev &P)
 {
-    void *ptrs[] = {P.xy, P.nu, P.bstart, P.sbucket, P.tstat, P.tdyn, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut,
-                    P.wq, P.fc, P.phibar, P.rbuf, P.lbuf, P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials, P.ticket, P.out, P.tmp, P.S, P.Sv,
-                    P.Yv, P.hval, P.hdiag, P.hbig_val, P.hcol, P.hcnt, P.hbig_col, P.herr, P.nb_b, P.nb_r, P.nb_z,
-                    P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.nb_tau, P.pcg, P.nst, P.nticket};
+    void *ptrs[] = {P.xy, P.nu, P.sbucket, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut, P.wq, P.fc, P.rbuf, P.lbuf,
+                    P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials,
+                    P.ticket, P.out, P.tmp, P.S, P.Sv, P.Yv, P.hval, P.hdiag, P.hbig_val, P.hcol, P.hcnt,
+                    P.hbig_col, P.herr, P.nb_b, P.nb_r, P.nb_z, P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.nb_tau, P.pcg,
+                    P.nst, P.nticket, P.bpart, P.bticket, P.bstat, P.cubtmp};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    P.xy = nullptr; P.nu = nullptr; P.sbucket = nullptr; P.rho = nullptr; P.perm = nullptr;
+    P.w = P.wt = P.d = P.mu = P.mut = P.wq = P.fc = nullptr;
+    P.rbuf = nullptr; P.lbuf = P.cstate = P.nv = P.ovf_list = P.ovf_list2 = P.ovf_count = nullptr;
+    P.nbc = P.nbn = P.nbc_q = P.nbn_q = nullptr;
+    P.partials = nullptr; P.ticket = nullptr; P.out = nullptr; P.tmp = nullptr; P.S = nullptr;
+    P.Sv = P.Yv = nullptr; P.hist_alloc = 0;
+    P.hval = P.hdiag = P.hbig_val = nullptr; P.hcol = P.hcnt = P.hbig_col = P.herr = nullptr; P.hbig_cap = 0;
+    P.nb_b = P.nb_r = P.nb_z = P.nb_pa = P.nb_pb = P.nb_q = P.nb_part = P.nb_tau = nullptr;
+    P.pcg = nullptr; P.nst = nullptr; P.nticket = nullptr;
+    P.bpart = nullptr; P.bticket = nullptr; P.bstat = nullptr; P.cubtmp = nullptr; P.cubtmp_bytes = 0;
+    P.cap_n = P.cap_pix = 0;
+}
+
+// The buffers sized by the bucket grid and the tree.
+static void free_sized_by_grid(CotProblemDev &P)
+{
+    void *ptrs[] = {P.bstart, P.tstat, P.tdyn, P.phibar};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    P.bstart = nullptr; P.tstat = P.tdyn = nullptr; P.phibar = nullptr;
+    P.cap_nb = P.cap_nodes = 0;
+}
+
+static void free_problem(CotProblemDev &P)
+{
+    free_sized_by_sites(P);
+    free_sized_by_grid(P);
     P = CotProblemDev();
 }
 
@@ -207,6 +245,7 @@ extern "C" int cot_create(const cot_config *cfg, cot_handle **out)
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hS, sizeof(CotSolver));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hN, sizeof(NewtonEvalStats));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hP, sizeof(PcgState));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->hB, 256);
     if (e != cudaSuccess) {
         if (h->hS) cudaFreeHost(h->hS);
         if (h->hN) cudaFreeHost(h->hN);
@@ -246,6 +285,7 @@ extern "C" int cot_destroy(cot_handle *h)
     if (h->hS) cudaFreeHost(h->hS);
     if (h->hN) cudaFreeHost(h->hN);
     if (h->hP) cudaFreeHost(h->hP);
+    if (h->hB) cudaFreeHost(h->hB);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return COT_OK;
@@ -299,73 +339,112 @@ extern "C" int cot_last_error(cot_handle *h, char *buf, size_t n)
     return COT_OK;
 }
 
-// Read caller data (host or device) into a host vector.
-static int to_host(cot_handle *h, const double *src, size_t count, int mem, std::vector<double> &dst)
-{
-    dst.resize(count);
-    if (count == 0) return COT_OK;
-    if (mem == COT_MEM_DEVICE) {
-        COT_CUDA_TRY(cudaMemcpyAsync(dst.data(), src, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
-    } else {
-        std::memcpy(dst.data(), src, count * sizeof(double));
-    }
-    return COT_OK;
-}
 
-// Build the device problem: bucket grid over the sites, counting sort
-// (bucket, then caller index), bound-tree statistics, density scaled to
-// sum(nu) per unit area.
-static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<double> &xy,
-                         const std::vector<double> &nu, const std::vector<double> &dens, int nx, int ny,
-                         const double pd[4])
+// Build the device problem (the kernels are in cot_build.cu): input checks
+// and sums, the bucket grid over the sites' box, the stable sort of the
+// sites by bucket (then caller index), the static bound tree, and the
+// density scaled to sum(nu) per unit area.  The host reads only the box and
+// the sums.  Inputs are host arrays (copied in first) or device arrays
+// (read in place) per mem.
+static int build_problem(cot_handle *h, CotProblemDev &P, const double *xy_in, const double *nu_in,
+                         const double *dens_in, int n, int nx, int ny, const double pd[4], int mem)
 {
-    const int n = (int)nu.size();
     cudaStream_t s = h->stream;
-    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
-    for (int i = 0; i < n; i++) {
-        double x = xy[2 * i], y = xy[2 * i + 1];
-        if (!std::isfinite(x) || !std::isfinite(y)) return failf(h, COT_EINVAL, "site %d is not finite", i);
-        xmin = std::min(xmin, x); xmax = std::max(xmax, x);
-        ymin = std::min(ymin, y); ymax = std::max(ymax, y);
+    const size_t npix = (size_t)nx * ny;
+    // ---- buffers sized by the sites and pixels (grow only) ---------------
+    if (!(P.xy != nullptr && (size_t)n <= P.cap_n && npix <= P.cap_pix)) {
+        free_sized_by_sites(P);
+        P.cap_n = (size_t)n;
+        P.cap_pix = npix;
+        const size_t N = P.cap_n;
+        cudaError_t e = cudaSuccess;
+        auto A = [&](void **p, size_t bytes) {
+            if (e == cudaSuccess) e = cudaMalloc(p, bytes > 0 ? bytes : 16);
+        };
+        A((void **)&P.xy, N * sizeof(double2));
+        A((void **)&P.nu, N * 8);
+        A((void **)&P.sbucket, N * sizeof(int));
+        A((void **)&P.rho, P.cap_pix * 8);
+        A((void **)&P.perm, N * sizeof(int));
+        A((void **)&P.w, N * 8);
+        A((void **)&P.wt, N * 8);
+        A((void **)&P.wq, N * 8);
+        A((void **)&P.rbuf, N * 32 * sizeof(double2));
+        A((void **)&P.lbuf, N * 32 * sizeof(int));
+        A((void **)&P.cstate, N * sizeof(int));
+        A((void **)&P.d, N * 8);
+        A((void **)&P.mu, N * 8);
+        A((void **)&P.mut, N * 8);
+        A((void **)&P.fc, N * 8);
+        A((void **)&P.nv, N * sizeof(int));
+        A((void **)&P.ovf_list, N * sizeof(int));
+        A((void **)&P.ovf_list2, N * sizeof(int));
+        A((void **)&P.ovf_count, 16 * sizeof(int));
+        A((void **)&P.nbc, N * COT_NBC * sizeof(int));
+        A((void **)&P.nbn, N * sizeof(int));
+        A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
+        A((void **)&P.nbn_q, N * sizeof(int));
+        A((void **)&P.partials, (size_t)reduce_blocks((int)N) * (5 * COT_MAX_HIST + 8) * 8);
+        A((void **)&P.ticket, sizeof(unsigned int));
+        A((void **)&P.out, sizeof(CotEvalOut));
+        A((void **)&P.tmp, 2 * N * 8);
+        A((void **)&P.S, sizeof(CotSolver));
+        A((void **)&P.bpart, build_partials_doubles() * 8);
+        A((void **)&P.bticket, 2 * sizeof(unsigned int));
+        A((void **)&P.bstat, 256);
+        if (e == cudaSuccess) e = cudaMemsetAsync(P.bticket, 0, 2 * sizeof(unsigned int), s);
+        if (e != cudaSuccess) {
+            free_sized_by_sites(P);
+            return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
+        }
     }
+    // ---- inputs on the device ------------------------------------------
+    const double *dxy = xy_in, *dnu = nu_in, *dd = dens_in;
+    if (mem == COT_MEM_HOST) {
+        // staging: raw sites in tmp, raw masses in mut, the raw density in
+        // rho (scaled there in place below)
+        COT_CUDA_TRY(cudaMemcpyAsync(P.tmp, xy_in, 2 * (size_t)n * 8, cudaMemcpyHostToDevice, s));
+        COT_CUDA_TRY(cudaMemcpyAsync(P.mut, nu_in, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+        COT_CUDA_TRY(cudaMemcpyAsync(P.rho, dens_in, npix * 8, cudaMemcpyHostToDevice, s));
+        dxy = P.tmp;
+        dnu = P.mut;
+        dd = P.rho;
+    }
+    // ---- checks, box and sums (one read back) ----------------------------
+    COT_CUDA_TRY(build_stats(n, dxy, dnu, (long long)npix, dd, P.bpart, P.bticket, P.bstat, P.bstat + 128, s));
+    COT_CUDA_TRY(cudaMemcpyAsync(h->hB, P.bstat, 256, cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaStreamSynchronize(s));
+    struct SiteStatsH {
+        double xmin, xmax, ymin, ymax, nusum;
+        long long bad_xy, bad_nu;
+    } ss;
+    struct DensStatsH {
+        double sum;
+        long long bad;
+    } ds;
+    std::memcpy(&ss, h->hB, sizeof ss);
+    std::memcpy(&ds, h->hB + 128, sizeof ds);
+    if (ss.bad_xy >= 0) return failf(h, COT_EINVAL, "site %lld is not finite", ss.bad_xy);
+    if (ss.bad_nu >= 0) return failf(h, COT_EINVAL, "cot_set_problem: nu[%lld] must be positive", ss.bad_nu);
+    if (ds.bad >= 0) return failf(h, COT_EINVAL, "density pixel %lld is negative or not finite", ds.bad);
+    if (!(ds.sum > 0)) return failf(h, COT_EINVAL, "density sums to zero");
+    // ---- the bucket grid and the tree's levels -----------------------------
+    const double xmin = ss.xmin, xmax = ss.xmax, ymin = ss.ymin, ymax = ss.ymax;
     double L = std::max({pd[1] - pd[0], pd[3] - pd[2], xmax - xmin, ymax - ymin,
                          std::fabs(pd[0]), std::fabs(pd[1]), std::fabs(pd[2]), std::fabs(pd[3])});
     if (!(L > 0)) L = 1.0;
     double wx = std::max(xmax - xmin, 1e-9 * L), wy = std::max(ymax - ymin, 1e-9 * L);
     wx *= 1.0 + 1e-12;
     wy *= 1.0 + 1e-12;
-    int bs = h->cfg.bucket_size;
-    double nbt = std::max(1.0, (double)n / bs);
+    const int bs = h->cfg.bucket_size;
+    const double nbt = std::max(1.0, (double)n / bs);
     int bx = std::max(1, (int)std::llround(std::sqrt(nbt * wx / wy)));
     int by = std::max(1, (int)std::llround(nbt / bx));
     bx = std::min(bx, 1 << 15);
     by = std::min(by, 1 << 15);
     const int nb = bx * by;
-    double hx = wx / bx, hy = wy / by;
-    double ihx = 1.0 / hx, ihy = 1.0 / hy;
-    std::vector<int> bucket(n), cnt(nb + 1, 0);
-    for (int i = 0; i < n; i++) {
-        int u = (int)((xy[2 * i] - xmin) * ihx), v = (int)((xy[2 * i + 1] - ymin) * ihy);
-        u = std::min(std::max(u, 0), bx - 1);
-        v = std::min(std::max(v, 0), by - 1);
-        bucket[i] = u + v * bx;
-        cnt[bucket[i] + 1]++;
-    }
-    for (int b = 0; b < nb; b++) cnt[b + 1] += cnt[b];
-    std::vector<int> cur(cnt.begin(), cnt.end() - 1), perm(n), sb(n);
-    for (int i = 0; i < n; i++) {
-        int p = cur[bucket[i]]++;
-        perm[p] = i;
-        sb[p] = bucket[i];
-    }
-    std::vector<double> sxy(2 * (size_t)n), snu(n);
-    for (int p = 0; p < n; p++) {
-        sxy[2 * p] = xy[2 * perm[p]];
-        sxy[2 * p + 1] = xy[2 * perm[p] + 1];
-        snu[p] = nu[perm[p]];
-    }
-    // tree statistics
+    const double hx = wx / bx, hy = wy / by;
+    const double ihx = 1.0 / hx, ihy = 1.0 / hy;
     std::vector<int> off, lw, lh;
     int W = bx, H = by, total = 0;
     while (true) {
@@ -379,127 +458,50 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const std::vector<doub
         if ((int)off.size() >= COT_MAX_LEVELS) return failf(h, COT_EINVAL, "too many tree levels");
     }
     const int nlev = (int)off.size();
-    // per node: the box of its sites {centre x, centre y, half width,
-    // half height}, widened by a relative 1e-12 (an empty node: half width -1)
-    std::vector<double4> tst(total);
-    auto boxed = [&](double x0, double x1, double y0, double y1) {
-        const double hx = 0.5 * (x1 - x0) * (1.0 + 1e-12) + 1e-15 * L;
-        const double hy = 0.5 * (y1 - y0) * (1.0 + 1e-12) + 1e-15 * L;
-        return make_double4(0.5 * (x0 + x1), 0.5 * (y0 + y1), hx, hy);
-    };
-    for (int b = 0; b < nb; b++) {
-        const int s0 = cnt[b], s1 = cnt[b + 1];
-        if (s1 <= s0) { tst[b] = make_double4(0.0, 0.0, -1.0, -1.0); continue; }
-        double x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
-        for (int p = s0; p < s1; p++) {
-            x0 = std::min(x0, sxy[2 * p]); x1 = std::max(x1, sxy[2 * p]);
-            y0 = std::min(y0, sxy[2 * p + 1]); y1 = std::max(y1, sxy[2 * p + 1]);
-        }
-        tst[b] = boxed(x0, x1, y0, y1);
-    }
-    for (int l = 1; l < nlev; l++) {
-        for (int v = 0; v < lh[l]; v++)
-            for (int u = 0; u < lw[l]; u++) {
-                double x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
-                for (int bb = 0; bb < 2; bb++)
-                    for (int aa = 0; aa < 2; aa++) {
-                        int uu = 2 * u + aa, vv = 2 * v + bb;
-                        if (uu >= lw[l - 1] || vv >= lh[l - 1]) continue;
-                        const double4 ch = tst[off[l - 1] + uu + vv * lw[l - 1]];
-                        if (ch.z < 0.0) continue;
-                        x0 = std::min(x0, ch.x - ch.z); x1 = std::max(x1, ch.x + ch.z);
-                        y0 = std::min(y0, ch.y - ch.w); y1 = std::max(y1, ch.y + ch.w);
-                    }
-                tst[off[l] + u + v * lw[l]] = x1 >= x0 ? boxed(x0, x1, y0, y1) : make_double4(0.0, 0.0, -1.0, -1.0);
-            }
-    }
-    // density per unit area, summing to sum(nu) over the domain
-    double area_scalar = 0, dsum = 0;
-    for (int i = 0; i < n; i++) area_scalar += nu[i];
-    for (size_t p = 0; p < dens.size(); p++) {
-        if (!std::isfinite(dens[p]) || dens[p] < 0) return failf(h, COT_EINVAL, "density pixel %zu is negative or not finite", p);
-        dsum += dens[p];
-    }
-    if (!(dsum > 0)) return failf(h, COT_EINVAL, "density sums to zero");
-    const double xs = (pd[1] - pd[0]) / (double)nx, ys = (pd[3] - pd[2]) / (double)ny;
-    const double ga = xs * ys;
-    const double gray = dsum / area_scalar;
-    std::vector<double> rho(dens.size());
-    for (size_t p = 0; p < dens.size(); p++) rho[p] = (dens[p] / gray) / ga;
-
-    // buffers grow only: a problem that fits the current ones reuses them
-    // (the Newton buffers and the history included); a larger one
-    // reallocates everything at its own sizes
-    const bool fits = P.xy != nullptr && (size_t)n <= P.cap_n && (size_t)nb <= P.cap_nb &&
-                      (size_t)total <= P.cap_nodes && rho.size() <= P.cap_pix;
-    if (!fits) {
-        free_problem(P);
-        P.cap_n = (size_t)n;
+    if (!(P.bstart != nullptr && (size_t)nb <= P.cap_nb && (size_t)total <= P.cap_nodes)) {
+        free_sized_by_grid(P);
         P.cap_nb = (size_t)nb;
         P.cap_nodes = (size_t)total;
-        P.cap_pix = rho.size();
+        cudaError_t e = cudaMalloc(&P.bstart, (P.cap_nb + 1) * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&P.tstat, P.cap_nodes * sizeof(double4));
+        if (e == cudaSuccess) e = cudaMalloc(&P.tdyn, P.cap_nodes * sizeof(double4));
+        if (e == cudaSuccess) e = cudaMalloc(&P.phibar, P.cap_nb * 8);
+        if (e != cudaSuccess) {
+            free_sized_by_grid(P);
+            return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
+        }
     }
     P.n = n;
     P.nb = nb;
     P.nodes = total;
-    P.hperm = perm;
     P.gen = ++g_problem_gen;
-    const size_t N = P.cap_n;
-    auto A = [&](void **p, size_t bytes) -> cudaError_t {
-        if (*p != nullptr) return cudaSuccess;  // reused
-        return cudaMalloc(p, bytes > 0 ? bytes : 16);
-    };
-    cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = A((void **)&P.xy, N * sizeof(double2));
-    if (e == cudaSuccess) e = A((void **)&P.nu, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.bstart, (P.cap_nb + 1) * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.sbucket, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.tstat, P.cap_nodes * sizeof(double4));
-    if (e == cudaSuccess) e = A((void **)&P.tdyn, P.cap_nodes * sizeof(double4));
-    if (e == cudaSuccess) e = A((void **)&P.rho, P.cap_pix * 8);
-    if (e == cudaSuccess) e = A((void **)&P.perm, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.w, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.wt, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.wq, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.phibar, P.cap_nb * 8);
-    if (e == cudaSuccess) e = A((void **)&P.rbuf, N * 32 * sizeof(double2));
-    if (e == cudaSuccess) e = A((void **)&P.lbuf, N * 32 * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.cstate, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.d, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.mu, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.mut, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.fc, N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.nv, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.ovf_list, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.ovf_list2, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.ovf_count, 16 * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.nbc, N * COT_NBC * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.nbn, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.nbn_q, N * sizeof(int));
-    if (e == cudaSuccess) e = A((void **)&P.partials, (size_t)reduce_blocks((int)P.cap_n) * (5 * COT_MAX_HIST + 8) * 8);
-    if (e == cudaSuccess) e = A((void **)&P.ticket, sizeof(unsigned int));
-    if (e == cudaSuccess) e = A((void **)&P.out, sizeof(CotEvalOut));
-    if (e == cudaSuccess) e = A((void **)&P.tmp, 2 * N * 8);
-    if (e == cudaSuccess) e = A((void **)&P.S, sizeof(CotSolver));
-    if (e != cudaSuccess) {
-        free_problem(P);
-        return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
+    // ---- the sort by bucket, the tree, the density -------------------------
+    size_t need = 0;
+    COT_CUDA_TRY(build_sort(n, dxy, dnu, xmin, ymin, ihx, ihy, bx, by, P.nv, P.ovf_list, P.ovf_list2, P.cstate,
+                            nullptr, &need, P.xy, P.nu, P.sbucket, P.perm, P.bstart, s));
+    if (need > P.cubtmp_bytes) {
+        if (P.cubtmp) cudaFree(P.cubtmp);
+        P.cubtmp = nullptr;
+        P.cubtmp_bytes = 0;
+        COT_CUDA_TRY(cudaMalloc(&P.cubtmp, need));
+        P.cubtmp_bytes = need;
     }
-    const size_t Nn = (size_t)n;  // the copies move this problem's sizes, not the capacities
-    COT_CUDA_TRY(cudaMemcpyAsync(P.xy, sxy.data(), Nn * sizeof(double2), cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.nu, snu.data(), Nn * 8, cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.bstart, cnt.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.sbucket, sb.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.tstat, tst.data(), total * sizeof(double4), cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice, s));
-    COT_CUDA_TRY(cudaMemcpyAsync(P.perm, perm.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, s));
+    need = P.cubtmp_bytes;
+    COT_CUDA_TRY(build_sort(n, dxy, dnu, xmin, ymin, ihx, ihy, bx, by, P.nv, P.ovf_list, P.ovf_list2, P.cstate,
+                            P.cubtmp, &need, P.xy, P.nu, P.sbucket, P.perm, P.bstart, s));
+    COT_CUDA_TRY(build_tree(nb, P.bstart, P.xy, L, nlev, off.data(), lw.data(), lh.data(), P.tstat, s));
+    const double xs = (pd[1] - pd[0]) / (double)nx, ys = (pd[3] - pd[2]) / (double)ny;
+    const double ga = xs * ys;
+    const double gray = ds.sum / ss.nusum;
+    COT_CUDA_TRY(build_density((long long)npix, dd, gray, ga, P.rho, s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ticket, 0, sizeof(unsigned int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 16 * sizeof(int), s));
-    COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, N * sizeof(int), s));
-    COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, N * sizeof(int), s));
-    if (P.hcnt) COT_CUDA_TRY(cudaMemsetAsync(P.hcnt, 0, N * sizeof(int), s));
-    COT_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above go out of scope
+    COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, P.cap_n * sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, P.cap_n * sizeof(int), s));
+    if (P.hcnt) COT_CUDA_TRY(cudaMemsetAsync(P.hcnt, 0, P.cap_n * sizeof(int), s));
+    P.hperm.resize(n);
+    COT_CUDA_TRY(cudaMemcpyAsync(P.hperm.data(), P.perm, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, s));
+    COT_CUDA_TRY(cudaStreamSynchronize(s));
 
     CotGeo &g = P.geo;
     g = CotGeo{};
@@ -546,15 +548,8 @@ extern "C" int cot_set_problem(cot_handle *h, const double *sites_xy, const doub
         !std::isfinite(pd[2]) || !std::isfinite(pd[3]))
         return fail(h, COT_EINVAL, "cot_set_problem: empty or non-finite proj_domain", nullptr);
     COT_CUDA_TRY(cudaSetDevice(h->device));
-    std::vector<double> xy, vnu, dens;
-    int r;
-    if ((r = to_host(h, sites_xy, 2 * (size_t)n, mem, xy)) != COT_OK) return r;
-    if ((r = to_host(h, nu, (size_t)n, mem, vnu)) != COT_OK) return r;
-    if ((r = to_host(h, density, (size_t)nx * ny, mem, dens)) != COT_OK) return r;
-    for (int i = 0; i < n; i++)
-        if (!(vnu[i] > 0) || !std::isfinite(vnu[i])) return failf(h, COT_EINVAL, "cot_set_problem: nu[%d] must be positive", i);
     h->has_problem = false;
-    r = build_problem(h, h->P, xy, vnu, dens, nx, ny, pd);
+    const int r = build_problem(h, h->P, sites_xy, nu, density, n, nx, ny, pd, mem);
     if (r != COT_OK) return r;
     h->has_problem = true;
     return COT_OK;
@@ -768,9 +763,10 @@ static int source_masses_impl(cot_handle *h, const double *points_xy, int n, con
 {
     COT_CUDA_TRY(cudaSetDevice(h->device));
     // unweighted cells inside the sample domain, one "pixel" of unit density
-    std::vector<double> xy(points_xy, points_xy + 2 * (size_t)n), one(n, 1.0), dens(1, 1.0);
+    std::vector<double> one(n, 1.0), dens(1, 1.0);
     CotProblemDev Q;
-    int r = build_problem(h, Q, xy, one, dens, 1, 1, sd);
+    int r = build_problem(h, Q, points_xy, one.data(), dens.data(), n, 1, 1, sd, COT_MEM_HOST);
+    if (r != COT_OK) free_problem(Q);
     if (r != COT_OK) return r;
     cudaStream_t s = h->stream;
     std::vector<double> val(n), sorted(n);

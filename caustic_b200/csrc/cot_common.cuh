@@ -185,6 +185,20 @@ void launch_reject_cond(cudaGraphConditionalHandle hc, CotSolver *S, CotCtx &c);
 void launch_init_from_eval(CotSolver *S, const CotEvalOut *out, CotCtx &c);
 void configure_cells_kernels();
 
+// Problem set-up on the device (cot_build.cu).  build_stats writes a
+// {xmin, xmax, ymin, ymax, sum nu, first bad site, first bad mass} record to
+// site_out and {sum, first bad pixel} to dens_out; build_sort with temp ==
+// nullptr only sets *temp_bytes.
+cudaError_t build_stats(int n, const double *xy, const double *nu, long long npix, const double *dens,
+                        double *partials, unsigned int *ticket, void *site_out, void *dens_out, cudaStream_t s);
+size_t build_partials_doubles();
+cudaError_t build_sort(int n, const double *xy, const double *nu, double ox, double oy, double ihx, double ihy,
+                       int bx, int by, int *keys, int *idx, int *keys2, int *idx2, void *temp, size_t *temp_bytes,
+                       double2 *sxy, double *snu, int *sbucket, int *perm, int *bstart, cudaStream_t s);
+cudaError_t build_tree(int nb, const int *bstart, const double2 *sxy, double L, int nlev, const int *off,
+                       const int *lw, const int *lh, double4 *tstat, cudaStream_t s);
+cudaError_t build_density(long long npix, const double *in, double gray, double ga, double *rho, cudaStream_t s);
+
 // Launchers implemented in cot_newton.cu (the Newton solve's kernels).
 struct NewtonEvalStats {
     double gnorm2;   // sum (mu - nu)^2

@@ -19,7 +19,10 @@
 
 One library handle per level is kept between calls: later problems of the
 same sizes reuse their device buffers (``cot_set_problem`` grows them only)
-and the trial-loop graph of the L-BFGS.  The reference has no counterpart:
+and the trial-loop graph of the L-BFGS.  The problem is copied to the GPU
+once; the coarser levels are built there (2 x 2 sums of sites, masses and
+pixels), the weights are interpolated there, and every level is handed to
+the library as device arrays, so that only the final weights come back.  The reference has no counterpart:
 its solver starts from the previous outer iteration's weights or from zero
 (main.cu:193-198).
 """
@@ -32,6 +35,30 @@ import numpy as np
 
 from . import capi, multilevel
 from .problems import SDOTProblem
+
+
+@dataclass
+class Level:
+    """Sizes of one level of a chain (its arrays live on the device)."""
+    n: int
+    grid: tuple
+    size: tuple
+    proj_domain: np.ndarray
+
+
+def chain_shapes(p: SDOTProblem, min_sites: int = 1024, max_levels: int = 8, min_pixels_per_site: int = 8) -> list:
+    """The levels multilevel.chain would build, sizes only, finest first."""
+    gx, gy = p.grid
+    W, H = p.size
+    out = [Level(p.n, (gx, gy), (W, H), np.asarray(p.proj_domain, np.float64))]
+    while len(out) <= max_levels:
+        if gx % 2 or gy % 2 or (gx // 2) * (gy // 2) < min_sites:
+            break
+        if W % 2 == 0 and H % 2 == 0 and W // (gx // 2) >= min_pixels_per_site and H // (gy // 2) >= min_pixels_per_site:
+            W, H = W // 2, H // 2
+        gx, gy = gx // 2, gy // 2
+        out.append(Level(gx * gy, (gx, gy), (W, H), out[0].proj_domain))
+    return out
 
 
 @dataclass
@@ -89,7 +116,7 @@ class WarmSolver:
         """The levels this pipeline solves, finest first."""
         if self.start == "zero":
             return [p]
-        ch = multilevel.chain(p, self.min_sites)
+        ch = chain_shapes(p, self.min_sites)
         if self.start == "learned" and self.learned_at == "level":
             keep = [q for q in ch if q.n >= self.net_level_sites]
             ch = keep if keep else ch[:1]
@@ -103,33 +130,94 @@ class WarmSolver:
                 return k
         return len(ch) - 1
 
+    def _device_chain(self, p: SDOTProblem):
+        """The chain's levels as device arrays: (descriptor, xy, nu,
+        picture) per level, finest first; the descriptors are SDOTProblems
+        without arrays (sizes, grid, domain)."""
+        import torch
+
+        dev = torch.device("cuda", self.device)
+        gx, gy = p.grid
+        W, H = p.size
+        xy = torch.from_numpy(np.ascontiguousarray(p.xy, np.float64)).to(dev).view(gy, gx, 2)
+        nu = torch.from_numpy(np.ascontiguousarray(p.nu, np.float64)).to(dev).view(gy, gx)
+        pic = torch.from_numpy(np.ascontiguousarray(p.picture, np.float64)).to(dev).view(H, W)
+        descs = self.chain(p)   # sizes only: the same rules as multilevel.chain
+        out = []
+        for k, q in enumerate(descs):
+            if k > 0:
+                # the 2 x 2 sums of multilevel.coarsen, in the same order
+                def s2(a):
+                    r = a[:, 0::2] + a[:, 1::2]
+                    return r[0::2] + r[1::2]
+
+                xy = 0.25 * s2(xy)
+                nu = s2(nu)
+                if tuple(q.size) != tuple(descs[k - 1].size):
+                    pic = s2(pic)
+            out.append((q, xy.reshape(-1).contiguous(), nu.reshape(-1).contiguous(), pic.reshape(-1).contiguous()))
+        return out
+
+    @staticmethod
+    def _prolong(w, coarse, fine_xy, fine):
+        """multilevel.prolong on device arrays."""
+        import torch
+
+        gxc, gyc = coarse.grid
+        d = np.asarray(fine.proj_domain, np.float64)
+        xy = fine_xy.view(-1, 2)
+        x = ((xy[:, 0] - d[0]) * (gxc / (d[1] - d[0])) - 0.5).clamp_(0.0, gxc - 1.0)
+        y = ((xy[:, 1] - d[2]) * (gyc / (d[3] - d[2])) - 0.5).clamp_(0.0, gyc - 1.0)
+        x0 = torch.clamp(x.to(torch.int64), max=max(gxc - 2, 0))
+        y0 = torch.clamp(y.to(torch.int64), max=max(gyc - 2, 0))
+        fx = x - x0
+        fy = y - y0
+        i00 = x0 + y0 * gxc
+        dx = 1 if gxc > 1 else 0
+        dy = gxc if gyc > 1 else 0
+        w00, w01, w10, w11 = w[i00], w[i00 + dx], w[i00 + dy], w[i00 + dx + dy]
+        a = w00 + fx * (w01 - w00)
+        b = w10 + fx * (w11 - w10)
+        r = a + fy * (b - a)
+        return r - r.mean()
+
     def solve(self, p: SDOTProblem):
         """(weights of ``p`` in its site order, WarmStats)."""
+        import torch
+
         t0 = time.perf_counter()
-        ch = self.chain(p)
+        ch = self._device_chain(p)
         chain_ms = 1e3 * (time.perf_counter() - t0)
+        dev = torch.device("cuda", self.device)
         infer_ms = 0.0
         if self.start == "learned":
             from . import warmstart
 
             ti = time.perf_counter()
-            k = self._net_level(ch)
-            w = warmstart.predict(self.net, [ch[k]])[0]
+            descs = [c[0] for c in ch]
+            k = self._net_level(descs)
+            q = descs[k]
+            # the network's inputs are host arrays of that level
+            qh = SDOTProblem(q.name, ch[k][1].view(-1, 2).cpu().numpy(), ch[k][2].cpu().numpy(),
+                             ch[k][3].cpu().numpy(), q.size, q.proj_domain, q.grid)
+            w = warmstart.predict(self.net, [qh])[0]
             if k != len(ch) - 1:
-                w = multilevel.restrict(w, ch[k], ch[-1])
+                qc = descs[-1]
+                w = multilevel.restrict(w, qh, qc)
+            w = torch.from_numpy(w).to(dev)
             infer_ms = 1e3 * (time.perf_counter() - ti)
         else:
-            w = np.zeros(ch[-1].n)
+            w = torch.zeros(ch[-1][0].n, dtype=torch.float64, device=dev)
         levels = []
         lwall = []
         dev_ms = 0.0
         for k in range(len(ch) - 1, -1, -1):
             tl = time.perf_counter()
-            q = ch[k]
+            q, xy, nu, pic = ch[k]
             if k < len(ch) - 1:
-                w = multilevel.prolong(w, ch[k + 1], q)
+                w = self._prolong(w, ch[k + 1][0], xy, q)
             s = self._handle(k)
-            s.set_problem(q.xy, q.nu, q.picture, q.size, q.proj_domain)
+            s.set_problem(xy, nu, pic, q.size, q.proj_domain)
             w, st = s.solve_newton(w, tol=self.tol if k == 0 else self.coarse_tol, history=self.history,
                                    shrink_steps=self.shrink_steps)
             levels.append((q.n, st))
@@ -139,5 +227,6 @@ class WarmSolver:
         w, js = self._handle(0).solve(w, mode=capi.SOLVE_WOLFE, tol=self.tol, history=self.history,
                                       max_iter=100000)
         dev_ms += js.ms
+        w = w.cpu().numpy()
         wall = 1e3 * (time.perf_counter() - t0)
         return w, WarmStats(bool(js.converged), js.max_rel_err, wall, dev_ms, infer_ms, levels, js, lwall, chain_ms)

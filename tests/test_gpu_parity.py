@@ -332,6 +332,38 @@ def test_torch_device_buffers(gpu):
     assert st.converged and wd.is_cuda
 
 
+def test_set_up_from_host_and_device_arrays_agree(gpu):
+    """cot_set_problem builds the problem on the device from host arrays
+    (copied in first) or device arrays (read in place): the same bits."""
+    import torch
+
+    p = problems.make(1, g=40, res=160, beam=True)
+    a = solver_for(p)
+    b = capi.Solver()
+    dev = torch.device("cuda", 0)
+    b.set_problem(torch.from_numpy(p.xy.reshape(-1)).to(dev), torch.from_numpy(p.nu).to(dev),
+                  torch.from_numpy(p.picture).to(dev), p.size, p.proj_domain)
+    w = np.random.default_rng(31).normal(0, 0.5 / p.n, p.n)
+    fa, mua, _, _ = a.eval(w)
+    fb, mub, _, _ = b.eval(w)
+    assert fa == fb and np.array_equal(mua, mub)
+    wa, sa = a.solve(np.zeros(p.n), tol=1e-4)
+    wb, sb = b.solve(np.zeros(p.n), tol=1e-4)
+    assert np.array_equal(wa, wb) and sa.evaluations == sb.evaluations
+    # a bad mass or pixel on the device is reported as on the host
+    nu = torch.from_numpy(p.nu).to(dev)
+    nu[17] = -1.0
+    with pytest.raises(capi.CotError) as e:
+        b.set_problem(torch.from_numpy(p.xy.reshape(-1)).to(dev), nu, torch.from_numpy(p.picture).to(dev), p.size,
+                      p.proj_domain)
+    assert "nu[17]" in str(e.value)
+    pic = p.picture.copy()
+    pic[99] = np.nan
+    with pytest.raises(capi.CotError) as e:
+        a.set_problem(p.xy, p.nu, pic, p.size, p.proj_domain)
+    assert "pixel 99" in str(e.value)
+
+
 def test_tiny_and_degenerate_inputs(gpu):
     """One site, two sites, sites on the domain boundary, a zero-density band."""
     dom = problems.UNIT_DOMAIN
