@@ -1872,8 +1872,9 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
             double sc = 1.0;
             for (int k = 0; k < o.shrink_steps; k++) {
                 sc *= 0.5;
-                double tau = sc - 1.0;
-                COT_CUDA_TRY(cudaMemcpyAsync(P.nb_tau, &tau, sizeof(double), cudaMemcpyHostToDevice, s));
+                double *ptau = reinterpret_cast<double *>(h->hB + 208);
+                *ptau = sc - 1.0;
+                COT_CUDA_TRY(cudaMemcpyAsync(P.nb_tau, ptau, sizeof(double), cudaMemcpyHostToDevice, s));
                 if ((rc = newton_eval(h, P.w)) != COT_OK) return finish(rc);
                 st.evaluations++;
                 if (h->hN->empty == 0) {
@@ -1921,26 +1922,28 @@ extern "C" int cot_solve_newton(cot_handle *h, double *w_inout, const cot_newton
                 st.converged = 1;
                 break;
             }
-            // the rings of the current point are the last evaluation's
-            int herr = 0;
-            COT_CUDA_TRY(cudaMemcpyAsync(&herr, P.herr, sizeof(int), cudaMemcpyDeviceToHost, s));
+            // the rings of the current point are the last evaluation's; one
+            // read back (pinned) for the long-row flag and the solve's state
+            int *herr = reinterpret_cast<int *>(h->hB + 200);
+            COT_CUDA_TRY(cudaMemcpyAsync(herr, P.herr, sizeof(int), cudaMemcpyDeviceToHost, s));
             launch_hessian(P.geo, P.rbuf, P.lbuf, P.nv, P.hval, P.hcol, P.hcnt, P.hdiag, h->c());
             k_rhs<<<nblk(P.n), 256, 0, s>>>(P.n, P.nu, P.mut, P.nb_b);
             h->ctx.launches++;
-            PcgState zero{};
-            COT_CUDA_TRY(cudaMemcpyAsync(P.pcg, &zero, sizeof zero, cudaMemcpyHostToDevice, s));
+            COT_CUDA_TRY(cudaMemsetAsync(P.pcg, 0, sizeof(PcgState), s));
             COT_CUDA_TRY(launch_pcg(P.n, P.hval, P.hcol, P.hcnt, P.hbig_val, P.hbig_col, P.hdiag, P.nb_b, P.d, P.nb_r,
                                     P.nb_z, P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.pcg, o.cg_rtol, o.cg_max_iter,
                                     pcg_blocks, h->c()));
             COT_CUDA_TRY(cudaMemcpyAsync(h->hP, P.pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
             COT_CUDA_TRY(cudaStreamSynchronize(s));
             st.cg_iterations += h->hP->iterations;
-            if (herr != 0 || h->hP->error != 0) break;  // the fall-back below finishes
+            if (*herr != 0 || h->hP->error != 0) break;  // the fall-back below finishes
             const double gn = std::sqrt(cur.gnorm2);
             double tau = 1.0;
             bool accepted = false;
+            double *ptau = reinterpret_cast<double *>(h->hB + 208);   // pinned: an asynchronous copy
             for (int ls = 0; ls < 30; ls++) {
-                COT_CUDA_TRY(cudaMemcpyAsync(P.nb_tau, &tau, sizeof(double), cudaMemcpyHostToDevice, s));
+                *ptau = tau;
+                COT_CUDA_TRY(cudaMemcpyAsync(P.nb_tau, ptau, sizeof(double), cudaMemcpyHostToDevice, s));
                 if ((rc = newton_eval(h, P.d)) != COT_OK) return finish(rc);
                 st.evaluations++;
                 const NewtonEvalStats t = *h->hN;

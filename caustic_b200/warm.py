@@ -77,7 +77,7 @@ class WarmStats:
 class WarmSolver:
     def __init__(self, start: str = "multilevel", net=None, net_level_sites: int = 0, min_sites: int = 1024,
                  tol: float = 1e-4, coarse_tol: float = 1e-3, history: int = 10, device: int = 0,
-                 learned_at: str = "coarsest", shrink_steps: int = 0):
+                 learned_at: str = "coarsest", shrink_steps: int = 0, shrink_coarsest: int = 0):
         if start not in ("multilevel", "learned", "zero"):
             raise ValueError(f"unknown start {start!r}")
         if start == "learned" and net is None:
@@ -85,7 +85,8 @@ class WarmSolver:
         if learned_at not in ("coarsest", "level"):
             raise ValueError(f"unknown learned_at {learned_at!r}")
         self.learned_at = learned_at
-        self.shrink_steps = shrink_steps
+        self.shrink_steps = shrink_steps          # scaled-down starts tried on every level
+        self.shrink_coarsest = shrink_coarsest    # ... and on the coarsest level only
         self.start = start
         self.net = net
         self.net_level_sites = net_level_sites
@@ -218,8 +219,9 @@ class WarmSolver:
                 w = self._prolong(w, ch[k + 1][0], xy, q)
             s = self._handle(k)
             s.set_problem(xy, nu, pic, q.size, q.proj_domain)
+            shrink = max(self.shrink_steps, self.shrink_coarsest if k == len(ch) - 1 else 0)
             w, st = s.solve_newton(w, tol=self.tol if k == 0 else self.coarse_tol, history=self.history,
-                                   shrink_steps=self.shrink_steps)
+                                   shrink_steps=shrink)
             levels.append((q.n, st))
             lwall.append(1e3 * (time.perf_counter() - tl))
             dev_ms += st.ms
