@@ -280,6 +280,17 @@ class Solver:
 
     def set_stream(self, stream_ptr: int):
         self._check(self._L.cot_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+        self._stream_ptr = int(stream_ptr or 0)
+
+    def _order_after_torch(self, t):
+        """Device tensors handed to the library were written on torch's
+        current stream; unless the handle runs on that same stream, wait for
+        it so that the library's stream reads them complete."""
+        import torch
+
+        cur = torch.cuda.current_stream(t.device)
+        if getattr(self, "_stream_ptr", 0) == 0 or cur.cuda_stream != self._stream_ptr:
+            cur.synchronize()
 
     # -------------------------------------------------------------------
     def set_problem(self, xy, nu, density, size, proj_domain):
@@ -288,6 +299,7 @@ class Solver:
         self._size = (nx, ny)
         pd = _f64(proj_domain)
         if _is_torch(xy):
+            self._order_after_torch(xy)
             self._check(self._L.cot_set_problem(self._h, _tptr(xy), _tptr(nu), int(nu.numel()), _tptr(density),
                                                 nx, ny, _dptr(pd), COT_MEM_DEVICE))
             self.n = int(nu.numel())
@@ -303,6 +315,8 @@ class Solver:
         f = ctypes.c_double()
         if _is_torch(w):
             import torch
+
+            self._order_after_torch(w)
             mu = torch.empty_like(w)
             g = torch.empty_like(w)
             fc = torch.empty_like(w)
@@ -338,6 +352,7 @@ class Solver:
         st = cot_solve_stats()
         if _is_torch(w0):
             w = w0.clone()
+            self._order_after_torch(w)
             rc = self._L.cot_solve(self._h, _tptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_DEVICE)
         else:
             w = _f64(w0).copy()
@@ -359,6 +374,7 @@ class Solver:
         st = cot_newton_stats()
         if _is_torch(w0):
             w = w0.clone()
+            self._order_after_torch(w)
             rc = self._L.cot_solve_newton(self._h, _tptr(w), ctypes.byref(opts), ctypes.byref(st), COT_MEM_DEVICE)
         else:
             w = _f64(w0).copy()
@@ -409,6 +425,8 @@ class Solver:
     def centroids(self, w, weighted=True):
         if _is_torch(w):
             import torch
+
+            self._order_after_torch(w)
             xy = torch.empty((self.n, 2), dtype=torch.float64, device=w.device)
             ex = torch.empty(self.n, dtype=torch.uint8, device=w.device)
             rc = self._L.cot_centroids(self._h, _tptr(w), _tptr(xy), _tptr(ex), int(bool(weighted)), COT_MEM_DEVICE)

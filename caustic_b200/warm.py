@@ -96,6 +96,7 @@ class WarmSolver:
         self.history = history
         self.device = device
         self._handles = {}
+        self._stream = None
 
     def close(self):
         for s in self._handles.values():
@@ -108,9 +109,21 @@ class WarmSolver:
     def __exit__(self, *a):
         self.close()
 
+    def _torch_stream(self):
+        """One stream for everything a solve does, the library's work and the
+        torch operations around it (levels, prolongation, inference), so that
+        each reads what the one before wrote."""
+        if self._stream is None:
+            import torch
+
+            self._stream = torch.cuda.Stream(device=torch.device("cuda", self.device))
+        return self._stream
+
     def _handle(self, k: int) -> capi.Solver:
         if k not in self._handles:
-            self._handles[k] = capi.Solver(device=self.device)
+            s = capi.Solver(device=self.device)
+            s.set_stream(self._torch_stream().cuda_stream)
+            self._handles[k] = s
         return self._handles[k]
 
     def chain(self, p: SDOTProblem) -> list:
@@ -184,6 +197,12 @@ class WarmSolver:
 
     def solve(self, p: SDOTProblem):
         """(weights of ``p`` in its site order, WarmStats)."""
+        import torch
+
+        with torch.cuda.stream(self._torch_stream()):
+            return self._solve(p)
+
+    def _solve(self, p: SDOTProblem):
         import torch
 
         t0 = time.perf_counter()
