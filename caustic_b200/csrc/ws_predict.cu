@@ -44,9 +44,21 @@ struct ws_net {
     double out_scale = 1.0;
     std::vector<int> ch;
     std::vector<Layer> layers;  // encoder convs, decoder convs, head
+    // device buffers of the last forward pass, reused while the site grid
+    // stays the same (a pass asks for the same buffers in the same order)
+    std::vector<void *> bufs;
+    std::vector<size_t> buf_bytes;
+    int grid_x = 0, grid_y = 0;
 };
 
 namespace {
+
+void free_bufs(ws_net *n)
+{
+    for (void *p : n->bufs) cudaFree(p);
+    n->bufs.clear();
+    n->buf_bytes.clear();
+}
 
 void free_net(ws_net *n)
 {
@@ -55,22 +67,35 @@ void free_net(ws_net *n)
         if (l.w16) cudaFree(l.w16);
         if (l.b) cudaFree(l.b);
     }
+    free_bufs(n);
     delete n;
 }
 
-// Device buffers of one forward pass, freed on scope exit.
+// Device buffers of a forward pass, handed out in request order from the
+// network's list: the k-th request of a pass reuses the k-th buffer when it is
+// large enough (the same grid asks for the same sizes), else it is replaced.
 struct Pool {
-    std::vector<void *> ptrs;
-    ~Pool()
-    {
-        for (void *p : ptrs) cudaFree(p);
-    }
+    ws_net *net;
+    size_t next = 0;
+    explicit Pool(ws_net *n) : net(n) {}
     template <class T>
     T *get(size_t count, cudaError_t &e)
     {
+        const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+        if (e != cudaSuccess) return nullptr;
+        if (next < net->bufs.size() && net->buf_bytes[next] >= bytes) return static_cast<T *>(net->bufs[next++]);
         void *p = nullptr;
-        if (e == cudaSuccess) e = cudaMalloc(&p, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
-        if (e == cudaSuccess) ptrs.push_back(p);
+        e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) return nullptr;
+        if (next < net->bufs.size()) {
+            cudaFree(net->bufs[next]);
+            net->bufs[next] = p;
+            net->buf_bytes[next] = bytes;
+        } else {
+            net->bufs.push_back(p);
+            net->buf_bytes.push_back(bytes);
+        }
+        next++;
         return static_cast<T *>(p);
     }
 };
@@ -212,7 +237,15 @@ extern "C" WS_API int cot_warmstart_predict(ws_net *net, const double *sites_xy,
             px[3] = __float2bfloat16_rn((float)lm);
         }
     // ---- forward pass (WarmStartNet.forward) ------------------------------
-    Pool pool;
+    if (net->grid_x != gx || net->grid_y != gy) {
+        // another grid: the earlier pass's buffers are released first (a
+        // buffer still being read by a pass in flight is not freed: the
+        // earlier pass ended with a synchronisation)
+        free_bufs(net);
+        net->grid_x = gx;
+        net->grid_y = gy;
+    }
+    Pool pool(net);
     cudaError_t e = cudaSuccess;
     auto *h = pool.get<__nv_bfloat16>(x.size(), e);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, x.data(), x.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, s);
