@@ -226,7 +226,7 @@ def warm_start_arms(args, p, cold_solve_ms, cold_e2e_ms, local):
     if os.path.exists(NET_C2):
         from caustic_b200 import warmstart
 
-        net = warmstart.WarmStartNet.from_file(NET_C2, device=f"cuda:{local}")
+        net = warmstart.CNet.from_npz(NET_C2, device=local)   # inference through the C ABI
         arms["learned"] = dict(start="learned", net=net, net_level_sites=NET_C2_LEVEL)
     out = {"cold_solve_ms": cold_solve_ms, "cold_e2e_ms": cold_e2e_ms,
            "timing": "host wall clock per whole solve (host arrays in, weights out), device synchronised; "

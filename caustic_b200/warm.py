@@ -218,9 +218,10 @@ class WarmSolver:
             k = self._net_level(descs)
             q = descs[k]
             # the network's inputs are host arrays of that level
-            qh = SDOTProblem(q.name, ch[k][1].view(-1, 2).cpu().numpy(), ch[k][2].cpu().numpy(),
+            qh = SDOTProblem(f"{p.name}/level{q.n}", ch[k][1].view(-1, 2).cpu().numpy(), ch[k][2].cpu().numpy(),
                              ch[k][3].cpu().numpy(), q.size, q.proj_domain, q.grid)
-            w = warmstart.predict(self.net, [qh])[0]
+            # the network through the C ABI (warmstart.CNet) or the Python host layer
+            w = self.net.predict(qh) if isinstance(self.net, warmstart.CNet) else warmstart.predict(self.net, [qh])[0]
             if k != len(ch) - 1:
                 qc = descs[-1]
                 w = multilevel.restrict(w, qh, qc)

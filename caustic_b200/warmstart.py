@@ -443,6 +443,18 @@ class CNet:
         if rc != 0:
             raise RuntimeError(f"cot_warmstart_load: {rc}: {self.error()}")
 
+    @classmethod
+    def from_npz(cls, npz_path: str, device: int = 0):
+        """Load a network saved by np.savez(**WarmStartNet.state_dict()):
+        written once more as the flat binary, then read through the C ABI."""
+        import tempfile
+
+        net = WarmStartNet.from_file(npz_path, device=f"cuda:{device}")
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "net.bin")
+            net.save_bin(path)
+            return cls(path, device)
+
     def error(self) -> str:
         buf = ctypes.create_string_buffer(512)
         self._L.cot_warmstart_last_error(buf, 512)
