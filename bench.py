@@ -677,6 +677,8 @@ def run_multilevel(args):
             "wall_speedup": tot["cold_wall"] / tot["ml_wall"],
             "cold_iterations_mean": float(np.mean([s.iterations for s in cold_st])),
             "cold_max_rel_err": float(max(s.max_rel_err for s in cold_st)),
+            "cold_converged": all(s.converged and s.max_rel_err <= args.tol for s in cold_st),
+            "multilevel_converged": all(s.converged and s.max_rel_err <= args.tol for s in ml_lv[-1].stats),
             "levels": [{"n_sites": lv.n, "image": list(lv.image), "tol": lv.tol, "ms": lv.ms,
                         "iterations_mean": float(np.mean([s.iterations for s in lv.stats])),
                         "max_rel_err": float(max(s.max_rel_err for s in lv.stats))} for lv in ml_lv],
