@@ -130,8 +130,10 @@ __device__ void ls_decide(CotSolver *S, const CotEvalOut &o)
     } else if (o.gtd > 0.0) {
         S->hi = t;
     } else {
+        // a step taken on the approximate conditions may sit a rounding
+        // above f_lo: it moves the bracket's low end but never raises f_lo
         S->lo = t;
-        S->f_lo = o.f;
+        S->f_lo = fmin(S->f_lo, o.f);
     }
     S->trials++;
     if (S->trials >= S->max_ls) {

@@ -591,7 +591,9 @@ def lbfgs_wolfe(prob: Problem, w0, tol=1e-4, m=10, max_iter=20000, c1=1e-4, c2=0
             elif gtd > 0:
                 hi = t
             else:
-                lo, f_lo, e_lo = t, e.f, e
+                # an approximate-Wolfe step may sit a rounding above f_lo:
+                # it moves lo but never raises f_lo (as cot_solver.cu)
+                lo, f_lo, e_lo = t, min(f_lo, e.f), e
             t = 2.0 * t if not np.isfinite(hi) else 0.5 * (lo + hi)
         if acc is None:
             if lo > 0:
