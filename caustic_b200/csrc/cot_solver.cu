@@ -105,6 +105,13 @@ __device__ void ls_decide(CotSolver *S, const CotEvalOut &o)
         if (S->t <= 1e-4 * S->t0) S->ls_active = 0;  // restart
         return;
     }
+    // a solve that only has to give every cell mass takes the first trial
+    // point where none is empty
+    if (S->stop_nonempty && o.empty == 0 && o.overflow == 0) {
+        S->accepted = 1;
+        S->ls_active = 0;
+        return;
+    }
     // strong Wolfe: bracket by doubling, zoom by bisection
     if (S->final_eval) {
         S->accepted = 1;
