@@ -205,8 +205,9 @@ def run_reference(args):
     return 0
 
 
-NET_C2 = os.path.join(ROOT, "caustic_b200", "data", "warmstart_c2.npz")
-NET_C2_LEVEL = 16384   # sites of the level the network predicts (128^2, 512^2 image at config 2)
+NET_C2 = os.path.join(ROOT, "caustic_b200", "data", "warmstart_c2_64.npz")
+NET_C2_LEVEL = 4096    # sites of the level the network predicts (64^2 sites, 256^2 image at config 2);
+                       # its prediction is averaged down to the coarsest level (1,024 sites)
 
 
 def warm_start_arms(args, p, cold_solve_ms, cold_e2e_ms, local):

@@ -12,7 +12,7 @@ from caustic_b200.warm import WarmSolver
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
-NET = os.path.join(os.path.dirname(warmstart.__file__), "data", "warmstart_c2.npz")
+NET = os.path.join(os.path.dirname(warmstart.__file__), "data", "warmstart_c2_64.npz")   # trained at 64^2 sites
 
 
 def oracle_err(p, w):
@@ -47,7 +47,7 @@ def test_learned_start_saves_damped_steps(gpu):
     L-BFGS and the oracle."""
     p = problems.make(2, 7)
     net = warmstart.WarmStartNet.from_file(NET)
-    with WarmSolver(start="multilevel") as ml, WarmSolver(start="learned", net=net, net_level_sites=16384) as le:
+    with WarmSolver(start="multilevel") as ml, WarmSolver(start="learned", net=net, net_level_sites=4096) as le:
         _, sm = ml.solve(p)
         w, sl = le.solve(p)
     assert sm.converged and sl.converged
