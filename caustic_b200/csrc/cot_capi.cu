@@ -44,7 +44,8 @@ struct CotProblemDev {
     // per evaluation
     double *w = nullptr, *wt = nullptr, *d = nullptr, *mu = nullptr, *mut = nullptr, *fc = nullptr;
     double *wq = nullptr;  // weights of the query entry points, apart from a solve's iterate w
-    double *phibar = nullptr;
+    double *wbar = nullptr;
+    int *blist = nullptr, *bcnt = nullptr;  // the bucket walk's leaf lists (solves only)
     double2 *rbuf = nullptr;  // ring vertices between the cell and integration kernels
     int *lbuf = nullptr;      // ring generators between the two ring-building kernels
     int *cstate = nullptr;    // per-cell state between them
@@ -192,10 +193,10 @@ static void free_sized_by_sites(CotProblemDev &P)
 // The buffers sized by the bucket grid and the tree.
 static void free_sized_by_grid(CotProblemDev &P)
 {
-    void *ptrs[] = {P.bstart, P.tstat, P.tdyn, P.phibar};
+    void *ptrs[] = {P.bstart, P.tstat, P.tdyn, P.wbar, P.blist, P.bcnt};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    P.bstart = nullptr; P.tstat = P.tdyn = nullptr; P.phibar = nullptr;
+    P.bstart = nullptr; P.tstat = P.tdyn = nullptr; P.wbar = nullptr; P.blist = P.bcnt = nullptr;
     P.cap_nb = P.cap_nodes = 0;
 }
 
@@ -465,7 +466,9 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const double *xy_in, c
         cudaError_t e = cudaMalloc(&P.bstart, (P.cap_nb + 1) * sizeof(int));
         if (e == cudaSuccess) e = cudaMalloc(&P.tstat, P.cap_nodes * sizeof(double4));
         if (e == cudaSuccess) e = cudaMalloc(&P.tdyn, P.cap_nodes * sizeof(double4));
-        if (e == cudaSuccess) e = cudaMalloc(&P.phibar, P.cap_nb * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&P.wbar, P.cap_nb * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&P.blist, P.cap_nb * COT_BLEAF * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&P.bcnt, P.cap_nb * sizeof(int));
         if (e != cudaSuccess) {
             free_sized_by_grid(P);
             return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
@@ -498,6 +501,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const double *xy_in, c
     COT_CUDA_TRY(cudaMemsetAsync(P.ovf_count, 0, 16 * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn, 0, P.cap_n * sizeof(int), s));
     COT_CUDA_TRY(cudaMemsetAsync(P.nbn_q, 0, P.cap_n * sizeof(int), s));
+    COT_CUDA_TRY(cudaMemsetAsync(P.bcnt, 0xff, P.cap_nb * sizeof(int), s));     // no bucket list yet
     if (P.hcnt) COT_CUDA_TRY(cudaMemsetAsync(P.hcnt, 0, P.cap_n * sizeof(int), s));
     P.hperm.resize(n);
     COT_CUDA_TRY(cudaMemcpyAsync(P.hperm.data(), P.perm, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -596,7 +600,7 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.d = d;
     a.tptr = tptr;
     a.wt = P.wt;
-    a.phibar = P.phibar;
+    a.wbar = P.wbar;
     a.rbuf = P.rbuf;
     a.lbuf = P.lbuf;
     a.cstate = P.cstate;
@@ -612,6 +616,9 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     const bool query = (w == P.wq);
     a.nbc = query ? P.nbc_q : P.nbc;
     a.nbn = query ? P.nbn_q : P.nbn;
+    // scratch of the bucket walk (rebuilt by every evaluation that uses it)
+    a.blist = P.blist;
+    a.bcnt = P.bcnt;
     return a;
 }
 

@@ -8,13 +8,14 @@
 // over the sites j that can reach it.  Working relative to s_i (x = s_i + x')
 // the half-plane of neighbour j is   e.x' <= (|e|^2 - (w_j - w_i)) / 2,
 // e = s_j - s_i.  Candidates come from the 3x3 neighbour buckets around s_i;
-// completeness is certified with plane bounds: writing phi_j = (|s_j|^2-w_j)/2
+// completeness is certified with a bound tree: writing phi_j = (|s_j|^2-w_j)/2
 // and P_j(x) = x.s_j - phi_j (cell i = where P_i is the largest), every tree
-// node holds {c, A, m, r} with  P_j(x) <= A + (x-c).m + |x-c| r  for all its
-// sites.  c is anchored where the node's cells lie (the local slope of phi),
-// so the bound stays tight when cells sit far from their sites.  A node whose
-// bound is below P_i at every vertex of the current polygon cannot cut the
-// cell (a convex bound minus a linear function peaks at a vertex).
+// node holds its sites' box and a weight bound {a, B} with w_j/2 <= a.s_j + B,
+// so that  P_j(x) <= (|x+a|^2 - dist(x+a, box)^2)/2 + B  for all its sites.
+// a is the local slope of the weights, so the bound stays tight when cells
+// sit far from their sites.  A node whose bound is below P_i at every vertex
+// of the current polygon cannot cut the cell (a convex bound minus a linear
+// function peaks at a vertex).
 //
 // The integration clips nothing: for each pixel of the cell's bounding box the
 // exact integrals of 1, x, y and |x-s_i|^2 over cell ∩ pixel are boundary sums
@@ -30,6 +31,7 @@ namespace cot {
 
 #define FULLMASK 0xffffffffu
 #define COT_FRMAX 96
+static_assert(COT_BLEAF <= COT_FRMAX && COT_BLEAF % 32 == 0, "a bucket list fits a frontier");
 
 #ifdef COT_PHASE_STATS
 // Measurement build only: per-phase cycle and event counters, kept per warp
@@ -57,21 +59,16 @@ __shared__ unsigned long long cot_pst[16][16];
 #define COT_RCAP 32  // ring buffer vertices per cell (the split integration)
 
 // ---------------------------------------------------------------------------
-// bucket and tree plane bounds (per evaluation)
+// bucket and tree weight bounds (per evaluation)
 // ---------------------------------------------------------------------------
 
-// phi_j = (|s_j|^2 - w_j) / 2 at the trial point w + t d, explicitly rounded so
-// that every thread that needs a bucket's mean computes the same bits.
+// w_j at the trial point w + t d, explicitly rounded so that every thread
+// that needs a bucket's mean computes the same bits.
 __device__ __forceinline__ double trial_weight(const double *__restrict__ w, const double *__restrict__ d, double t,
                                                int j)
 {
     // no contraction: the trial point is w + t*d exactly as written
     return d != nullptr ? __dadd_rn(w[j], __dmul_rn(t, d[j])) : w[j];
-}
-
-__device__ __forceinline__ double half_phi(double2 s, double wj)
-{
-    return __dmul_rn(0.5, __dsub_rn(__fma_rn(s.x, s.x, __dmul_rn(s.y, s.y)), wj));
 }
 
 // The bucket kernels work one bucket per 16-lane segment (a half warp):
@@ -95,7 +92,7 @@ __device__ __forceinline__ double bseg_max(double v, unsigned m)
 // bucket).  Block 0 also clears the cell kernels' counters.
 __global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const double *__restrict__ d,
                              const double *__restrict__ tptr, double *__restrict__ wt,
-                             double *__restrict__ phibar, int *counters, int ncounters)
+                             double *__restrict__ wbar, int *counters, int ncounters)
 {
     if (blockIdx.x == 0 && (int)threadIdx.x < ncounters) counters[threadIdx.x] = 0;
     const int b = (blockIdx.x * blockDim.x + threadIdx.x) / BSEG;
@@ -108,23 +105,23 @@ __global__ void k_bucket_phi(CotGeo g, const double *__restrict__ w, const doubl
     for (int j = s0 + sl; j < s1; j += BSEG) {
         const double wj = trial_weight(w, d, t, j);
         wt[j] = wj;
-        acc = __dadd_rn(acc, half_phi(g.xy[j], wj));
+        acc = __dadd_rn(acc, wj);
     }
     acc = bseg_sum(acc, m);
-    if (sl == 0) phibar[b] = (s1 > s0) ? acc / (double)(s1 - s0) : 0.0;
+    if (sl == 0) wbar[b] = (s1 > s0) ? 0.5 * acc / (double)(s1 - s0) : 0.0;
 }
 
-// Plane bound of bucket b: c_b = slope of phi across the neighbouring buckets
-// (central difference of their mean phi over their box centres, one-sided at
-// the grid edges), A_b = max_j c_b.s_j - phi_j.  Called by a whole segment
-// (mask msk); every lane returns the bound.
+// Weight bound of bucket b: a_b = slope of w/2 across the neighbouring
+// buckets (central difference of their mean w/2 over their box centres,
+// one-sided at the grid edges), B_b = max_j w_j/2 - a_b.s_j.  Called by a
+// whole segment (mask msk); every lane returns the bound.
 __device__ __forceinline__ double4 bucket_bound(const CotGeo &g, const double *__restrict__ wt,
-                                                const double *__restrict__ phibar, int b, int sl, unsigned msk)
+                                                const double *__restrict__ wbar, int b, int sl, unsigned msk)
 {
     const double4 st = g.tstat[b];
     if (st.z < 0.0) return make_double4(0.0, 0.0, -INFINITY, 0.0);
     const int u = b % g.bx, v = b / g.bx;
-    const double pb = phibar[b];
+    const double pb = wbar[b];
     double c[2];
     for (int ax = 0; ax < 2; ax++) {
         int bp = -1, bm = -1;
@@ -140,38 +137,38 @@ __device__ __forceinline__ double4 bucket_bound(const CotGeo &g, const double *_
         if (bp >= 0 && bm >= 0) {
             const double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
             const double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
-            val = (phibar[bp] - phibar[bm]) / (mp - mm);
+            val = (wbar[bp] - wbar[bm]) / (mp - mm);
         } else if (bp >= 0) {
             const double mp = ax == 0 ? g.tstat[bp].x : g.tstat[bp].y;
-            val = (phibar[bp] - pb) / (mp - mb);
+            val = (wbar[bp] - pb) / (mp - mb);
         } else if (bm >= 0) {
             const double mm = ax == 0 ? g.tstat[bm].x : g.tstat[bm].y;
-            val = (pb - phibar[bm]) / (mb - mm);
+            val = (pb - wbar[bm]) / (mb - mm);
         } else {
-            val = mb;
+            val = 0.0;
         }
-        if (!isfinite(val)) val = mb;
+        if (!isfinite(val)) val = 0.0;
         c[ax] = val;
     }
-    double A = -INFINITY;
+    double B = -INFINITY;
     const int s0 = g.bstart[b], s1 = g.bstart[b + 1];
     for (int j = s0 + sl; j < s1; j += BSEG) {
         const double2 s = g.xy[j];
-        A = fmax(A, c[0] * s.x + c[1] * s.y - half_phi(s, wt[j]));
+        B = fmax(B, 0.5 * wt[j] - (c[0] * s.x + c[1] * s.y));
     }
-    A = bseg_max(A, msk);
-    return make_double4(c[0], c[1], A, 0.0);
+    B = bseg_max(B, msk);
+    return make_double4(c[0], c[1], B, 0.0);
 }
 
-// Bucket plane bounds, one bucket per segment.
+// Bucket weight bounds, one bucket per segment.
 #define TREE_THREADS 256
 __global__ void __launch_bounds__(TREE_THREADS) k_tree_build(CotGeo g, const double *__restrict__ wt,
-                                                            const double *__restrict__ phibar)
+                                                            const double *__restrict__ wbar)
 {
     const int b = (blockIdx.x * blockDim.x + threadIdx.x) / BSEG;
     const int sl = threadIdx.x & (BSEG - 1);
     if (b >= g.bx * g.by) return;  // whole segments leave together
-    const double4 bd = bucket_bound(g, wt, phibar, b, sl, bseg_mask());
+    const double4 bd = bucket_bound(g, wt, wbar, b, sl, bseg_mask());
     if (sl == 0) g.tdyn[b] = bd;
 }
 
@@ -204,9 +201,9 @@ __device__ __forceinline__ double tree_block_max(double v, double *sh)
 
 // Tree levels 1..lmax (the levels a certificate walk can start from; the
 // ones above are never read), one block per node, each straight from the
-// buckets and sites under it: c = the mean slope point of its non-empty
-// buckets, A = max_j c.s_j - phi_j over its sites, the exact value at c.
-// No level waits for the one below, and no bound is a bound of bounds.
+// buckets and sites under it: a = the mean weight slope of its non-empty
+// buckets, B = max_j w_j/2 - a.s_j over its sites, the exact value for that
+// a.  No level waits for the one below, and no bound is a bound of bounds.
 __global__ void __launch_bounds__(TREE_THREADS) k_tree_levels(CotGeo g, const double *__restrict__ wt)
 {
     __shared__ double sh[TREE_THREADS / 32];
@@ -235,17 +232,17 @@ __global__ void __launch_bounds__(TREE_THREADS) k_tree_levels(CotGeo g, const do
     sy = tree_block_sum(sy, sh);
     sc = tree_block_sum(sc, sh);
     const double cx = sx / sc, cy = sy / sc;
-    double A = -INFINITY;
+    double B = -INFINITY;
     for (int v = v0; v < v1; v++) {
         // the rectangle's buckets in one row hold consecutive sites
         const int j0 = g.bstart[u0 + v * g.bx], j1 = g.bstart[u1 + v * g.bx];
         for (int j = j0 + threadIdx.x; j < j1; j += TREE_THREADS) {
             const double2 s2 = g.xy[j];
-            A = fmax(A, cx * s2.x + cy * s2.y - half_phi(s2, wt[j]));
+            B = fmax(B, 0.5 * wt[j] - (cx * s2.x + cy * s2.y));
         }
     }
-    A = tree_block_max(A, sh);
-    if (threadIdx.x == 0) g.tdyn[node] = make_double4(cx, cy, A, 0.0);
+    B = tree_block_max(B, sh);
+    if (threadIdx.x == 0) g.tdyn[node] = make_double4(cx, cy, B, 0.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -546,27 +543,33 @@ __device__ int clip_chunk(WarpPoly<MAXV> &P, int nv, int j, const CotGeo &g, dou
     return nv;
 }
 
-// Can no site of `node` beat site i anywhere on the current polygon?  For
-// every site j of the node, P_j(x) = x.s_j - phi_j <= A + (x - c).m +
-// |x - c|_x h_x + |x - c|_y h_y (c, A: the node's plane bound, m, h: the
-// centre and half extents of its sites' box); the node is excluded when that
-// stays below P_i - margin at every vertex (a convex bound minus a linear
-// function peaks at a vertex).
+// Can no site of `node` beat site i anywhere on the current polygon?  With
+// P_j(x) = x.s_j - phi_j, phi_j = (|s_j|^2 - w_j)/2, and the node's weight
+// bound (a, B: w_j/2 <= a.s_j + B for each of its sites j),
+//     P_j(x) = (x + a).s_j - |s_j|^2/2 + (w_j/2 - a.s_j) <= F(x + a) + B,
+//     F(y) = max over the node's site box of y.s - |s|^2/2
+//          = (|y|^2 - dist(y, box)^2) / 2,
+// F being convex (a maximum of affine functions of y).  The node is excluded
+// when F(x + a) + B + margin <= P_i(x) at every vertex x of the polygon: a
+// convex function minus an affine one peaks at a vertex.  With x = s_i + v
+// (v in the site's frame) and t = v + a the condition reads
+//     |t|^2 + 2 (s_i.a + B + margin) - w_i <= dist(s_i + t, box)^2.
+// The quadratic is exact where a plane bound of phi would lose h^2/2 for a
+// node of half width h.
 template <class SP>
 __device__ __forceinline__ bool node_excluded(const SP &P, int nv, const CotGeo &g, int node,
-                                              double2 si, double halfs2w)
+                                              double2 si, double wi)
 {
-    double4 st = g.tstat[node];
+    const double4 st = g.tstat[node];
     if (st.z < 0.0) return true;
-    double4 dy = g.tdyn[node];
-    double qx = si.x - dy.x, qy = si.y - dy.y;
-    double gx = st.x - si.x, gy = st.y - si.y;
-    double K = dy.z + qx * st.x + qy * st.y - halfs2w;
+    const double4 dy = g.tdyn[node];
+    const double px = si.x - st.x + dy.x, py = si.y - st.y + dy.y;
+    const double C = 2.0 * (si.x * dy.x + si.y * dy.y + dy.z + g.margin) - wi;
     for (int k = 0; k < nv; k++) {
-        double x = P.X[k], y = P.Y[k];
-        double R = -g.margin - K - (x * gx + y * gy);
-        double ux = qx + x, uy = qy + y;
-        if (!(R > fabs(ux) * st.z + fabs(uy) * st.w)) return false;
+        const double tx = P.X[k] + dy.x, ty = P.Y[k] + dy.y;
+        const double ex = fmax(fabs(P.X[k] + px) - st.z, 0.0);
+        const double ey = fmax(fabs(P.Y[k] + py) - st.w, 0.0);
+        if (!(__fma_rn(tx, tx, __fma_rn(ty, ty, C)) <= __fma_rn(ex, ex, ey * ey))) return false;
     }
     return true;
 }
@@ -1626,7 +1629,6 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
     const int bu = bi % g.bx, bv = bi / g.bx;
     const int win = cached ? -1 : COT_WIN;
     // ---- 2. certificate over the bound tree --------------------------------
-    const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
     bool brute = false;
     if (ok && P.nv > 0 && g.nlev > 0) {
         if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
@@ -1642,13 +1644,40 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
         int ncur = g.lev_w[top] * g.lev_h[top];
         if (ncur > COT_FRMAX) brute = true;
         int cur = 0;
-        if (!brute) {
+        bool have = false;  // the surviving leaves are in S.fr[cur][0, ncur)
+        if constexpr (LPC == 32) {
+            // the leaf buckets k_bucket_walk listed for the cell's bucket: one
+            // round of leaf tests against this ring, in the walk's order
+            if (!brute && a.bcnt != nullptr) {
+                const int bc = a.bcnt[bi];
+                if (bc >= 0) {
+                    int nl = 0;
+                    for (int base = 0; base < bc; base += LPC) {
+                        const int e = base + lane < bc ? a.blist[(size_t)bi * COT_BLEAF + base + lane] : -1;
+                        bool keep = false;
+                        if (e >= 0) {
+                            const int u = e % g.bx, v = e / g.bx;
+                            const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
+                            keep = !inwin && !node_excluded(S, nv0, g, e, si, wi);
+                        }
+                        const unsigned m = SG.ballot(keep);
+                        if (keep) S.fr[1][nl + __popc(m & ((1u << lane) - 1u))] = e;
+                        nl += __popc(m);
+                    }
+                    SG.sync();
+                    ncur = nl;
+                    cur = 1;
+                    have = true;
+                }
+            }
+        }
+        if (!brute && !have) {
             // frontier entries are packed node coordinates u | v << 16
             const int tw = g.lev_w[top];
             for (int q = lane; q < ncur; q += LPC) S.fr[0][q] = (q % tw) | ((q / tw) << 16);
             SG.sync();
         }
-        for (int L = top; L >= 0 && !brute; L--) {
+        for (int L = top; L >= 0 && !brute && !have; L--) {
             int nnext = 0;
             const int off = g.lev_off[L], W = g.lev_w[L];
             PSTAT_ADD(7, ncur);
@@ -1660,7 +1689,7 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
                     u = q & 0xffff;
                     v = q >> 16;
                     const bool inwin = L == 0 && abs(u - bu) <= win && abs(v - bv) <= win;
-                    keep = !inwin && !node_excluded(S, nv0, g, off + u + v * W, si, halfs2w);
+                    keep = !inwin && !node_excluded(S, nv0, g, off + u + v * W, si, wi);
                 }
                 if (L == 0) {
                     const unsigned m = SG.ballot(keep);
@@ -1719,7 +1748,7 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
             if (b < nb) {
                 const int u = b % g.bx, v = b / g.bx;
                 const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
-                keep = !inwin && !node_excluded(S, P.nv, g, b, si, halfs2w);
+                keep = !inwin && !node_excluded(S, P.nv, g, b, si, wi);
             }
             SG.sync();
             int st = 0, cnt = 0;
@@ -1941,6 +1970,118 @@ __global__ void __launch_bounds__(128, MINB) k_cells_first(CotGeo g, CellsArgs a
     PSTAT_FLUSH();
 }
 
+// One warp per bucket, between k_cells_first and k_cells_walk: the leaf
+// buckets whose sites could cut the ring of any cell of the bucket.  The
+// rings phase 1 left lie in a box; with i0 the bucket's first site and
+// Delta = max over the rings' vertices of P_i0 - P_i (P_i0 - P_i is affine on
+// a ring, so its vertices bound it), P_i0 - Delta <= P_i on ring i.  A node
+// whose bound stays below P_i0 - Delta - margin at the box's four corners
+// (node_excluded with w_i0 - 2 Delta) therefore cuts no ring of the bucket.
+// The surviving leaves are listed in walk order (COT_BLEAF at most; -1 when
+// more), so that k_cells_walk tests only them, in one or two rounds a cell.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_bucket_walk(CotGeo g, CellsArgs a)
+{
+    constexpr int LPC = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int nb = g.bx * g.by;
+    int *fetch = a.ovf_count + 9;
+    int top = g.nlev - 1;
+    while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= 32) top--;
+    const int ntop = g.lev_w[top] * g.lev_h[top];
+    while (true) {
+        int b = 0;
+        if (lane == 0) b = atomicAdd(fetch, 1);
+        b = __shfl_sync(FULLMASK, b, 0);
+        if (b >= nb) break;
+        const int s0 = g.bstart[b], s1 = g.bstart[b + 1];
+        const double2 so = s1 > s0 ? g.xy[s0] : make_double2(0.0, 0.0);
+        const double wo = s1 > s0 ? a.wt[s0] : 0.0;
+        double lx = INFINITY, hx = -INFINITY, ly = INFINITY, hy = -INFINITY, dl = 0.0;
+        for (int i = s0 + lane; i < s1; i += 32) {
+            const int st = a.cstate[i];
+            if (st < 0) continue;
+            const int nv = st & 0xff;
+            const double2 si = g.xy[i];
+            const double ex = si.x - so.x, ey = si.y - so.y;
+            // P_i0 - P_i at s_i + v: (w_i0 - w_i)/2 - |e|^2/2 - v.e, e = s_i - s_i0
+            const double k0 = 0.5 * (wo - a.wt[i]) - 0.5 * __fma_rn(ex, ex, ey * ey);
+            for (int k = 0; k < nv; k++) {
+                const double2 v = a.rbuf[(size_t)i * COT_RCAP + k];
+                const double X = v.x + ex, Y = v.y + ey;
+                lx = fmin(lx, X);
+                hx = fmax(hx, X);
+                ly = fmin(ly, Y);
+                hy = fmax(hy, Y);
+                dl = fmax(dl, k0 - __fma_rn(v.x, ex, v.y * ey));
+            }
+        }
+        lx = warp_min(lx);
+        hx = warp_max(hx);
+        ly = warp_min(ly);
+        hy = warp_max(hy);
+        dl = warp_max(dl);
+        if (!(lx <= hx)) {
+            // no ring of the bucket is walked
+            if (lane == 0) a.bcnt[b] = 0;
+            continue;
+        }
+        if (lane < 4) {
+            S.X[lane] = (lane == 1 || lane == 2) ? hx : lx;
+            S.Y[lane] = lane >= 2 ? hy : ly;
+        }
+        for (int q = lane; q < ntop; q += 32) S.fr[0][q] = (q % g.lev_w[top]) | ((q / g.lev_w[top]) << 16);
+        __syncwarp();
+        const double wq = wo - 2.0 * dl;
+        int cur = 0, ncur = ntop;
+        bool over = ntop > COT_FRMAX;
+        for (int L = top; L >= 0 && !over; L--) {
+            int nnext = 0;
+            const int off = g.lev_off[L], W = g.lev_w[L];
+            for (int base = 0; base < ncur; base += 32) {
+                const int q = (base + lane < ncur) ? S.fr[cur][base + lane] : -1;
+                bool keep = false;
+                int u = 0, v = 0;
+                if (q >= 0) {
+                    u = q & 0xffff;
+                    v = q >> 16;
+                    keep = !node_excluded(S, 4, g, off + u + v * W, so, wq);
+                }
+                if (L == 0) {
+                    const unsigned m = __ballot_sync(FULLMASK, keep);
+                    const int cnt = __popc(m);
+                    if (nnext + cnt > COT_BLEAF) { over = true; break; }
+                    if (keep) S.fr[1 - cur][nnext + __popc(m & ((1u << lane) - 1u))] = u + v * W;
+                    nnext += cnt;
+                } else {
+                    const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1];
+                    const int chc = keep ? (2 * u + 1 < cw ? 2 : 1) * (2 * v + 1 < ch ? 2 : 1) : 0;
+                    const int inc = warp_incl_scan(chc, lane);
+                    const int cnt = __shfl_sync(FULLMASK, inc, 31);
+                    if (nnext + cnt > COT_FRMAX) { over = true; break; }
+                    int pos = nnext + inc - chc;
+                    if (keep) {
+                        for (int bb = 0; bb < 2; bb++)
+                            for (int aa = 0; aa < 2; aa++)
+                                if (2 * u + aa < cw && 2 * v + bb < ch) S.fr[1 - cur][pos++] = (2 * u + aa) | ((2 * v + bb) << 16);
+                    }
+                    nnext += cnt;
+                }
+            }
+            __syncwarp();
+            if (over) break;
+            cur = 1 - cur;
+            ncur = nnext;
+        }
+        if (!over)
+            for (int k = lane; k < ncur; k += 32) a.blist[(size_t)b * COT_BLEAF + k] = S.fr[cur][k];
+        if (lane == 0) a.bcnt[b] = over ? -1 : ncur;
+        __syncwarp();
+    }
+}
+
 // KEEP: leave the final ring's generators in lbuf (the Newton solve's
 // Jacobian reads them); a separate instance keeps the solve's path as it is.
 template <int MINB, bool KEEP>
@@ -2114,8 +2255,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
         PSTAT_ADD(0, t1 - t0);
         PSTAT_ADD(10, cached ? 1 : 0);
         // ---- 2. certificate over the bound tree --------------------------------
-        const double halfs2w = 0.5 * (si.x * si.x + si.y * si.y) + 0.5 * wi;
-        bool brute = false;
+            bool brute = false;
         if (nv > 0 && status == 0 && g.nlev > 0) {
             int top = g.nlev - 1;
             while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= 32) top--;
@@ -2137,9 +2277,9 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
                         if (L == 0) {
                             int u = q % W, v = q / W;
                             bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
-                            keep = !inwin && !node_excluded(P, nv, g, off + q, si, halfs2w);
+                            keep = !inwin && !node_excluded(P, nv, g, off + q, si, wi);
                         } else {
-                            keep = !node_excluded(P, nv, g, off + q, si, halfs2w);
+                            keep = !node_excluded(P, nv, g, off + q, si, wi);
                         }
                     }
                     if (L == 0) {
@@ -2199,7 +2339,7 @@ __global__ void __launch_bounds__(128, MINB) k_cells(CotGeo g, CellsArgs a, int 
                 if (b < nb) {
                     int u = b % g.bx, v = b / g.bx;
                     bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
-                    keep = !inwin && !node_excluded(P, nv, g, b, si, halfs2w);
+                    keep = !inwin && !node_excluded(P, nv, g, b, si, wi);
                 }
                 unsigned m = __ballot_sync(FULLMASK, keep);
                 while (m != 0u && nv > 0 && status == 0) {
@@ -2354,7 +2494,7 @@ static size_t cells_smem(int maxv, int warps)
 #define WALK_MINB 8   // k_cells_walk (64 registers; 6 blocks measured 2 % slower)
 #endif
 static int g_blocks_per_sm32 = 0, g_blocks_per_sm16 = 0, g_blocks_per_sm8 = 0, g_blocks_per_smi = 0;
-static int g_blocks_per_smf = 0, g_blocks_per_smw = 0;
+static int g_blocks_per_smf = 0, g_blocks_per_smw = 0, g_blocks_per_smb = 0;
 
 template <bool EXACT, int LPC>
 static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int blocks, cudaStream_t s)
@@ -2367,19 +2507,21 @@ static void launch_fast(const CotGeo &g, const CellsArgs &a, int pass, int block
 // (4) runs the hot path on 16-lane (8-lane) segments, two (four) cells per
 // warp, with a 32-lane second pass for rings above 16 (8) vertices; every
 // path ends with the 256-vertex pass for rings above 32.
-void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms, CotCtx &c)
+void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int num_sms, CotCtx &c)
 {
     cudaStream_t s = c.s;
+    CellsArgs a = args;
     const int nb = g.bx * g.by;
     // tree levels up to the first one of at most 16 nodes: the highest level
     // any certificate walk starts from (one round of a 16- or 32-lane segment)
     int lmax = 0;
     while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
     // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
-    // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter
+    // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter,
+    // [9]: k_bucket_walk's
     const int segs = (nb * BSEG + 127) / 128;
-    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.phibar, a.ovf_count, 9);
-    k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.phibar);
+    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 10);
+    k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.wbar);
     c.launches += 2;
     int upper = 0;  // nodes of levels 1..lmax
     for (int L = 1; L <= lmax; L++) upper += g.lev_w[L] * g.lev_h[L];
@@ -2390,6 +2532,9 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
     const int sms = num_sms > 0 ? num_sms : 148;
     const bool exact = a.cen != nullptr || a.splat != nullptr || a.solid != nullptr;
     const int lpc = (exact || cells_per_warp < 2) ? 32 : (cells_per_warp == 2 ? 16 : 8);
+    // the bucket walk's lists exist only on the path that runs it: every
+    // other path walks in full
+    if (exact || lpc != 32) a.blist = a.bcnt = nullptr;
     const int per_sm32 = g_blocks_per_sm32 > 0 ? g_blocks_per_sm32 : CELLS_MINB;
     const int per_sm16 = g_blocks_per_sm16 > 0 ? g_blocks_per_sm16 : CELLS_MINB;
     const int per_sm8 = g_blocks_per_sm8 > 0 ? g_blocks_per_sm8 : 1;
@@ -2405,6 +2550,11 @@ void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int nu
         const int bf = std::min(g.n, sms * (g_blocks_per_smf > 0 ? g_blocks_per_smf : FIRST_MINB) * CELLS_WPB);
         const size_t sm = sizeof(FastScratch) * CELLS_WPB;
         k_cells_first<FIRST_MINB><<<(bf + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+        if (a.bcnt != nullptr) {
+            const int bb = std::min(nb, sms * (g_blocks_per_smb > 0 ? g_blocks_per_smb : WALK_MINB) * CELLS_WPB);
+            k_bucket_walk<WALK_MINB><<<(bb + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+            c.launches++;
+        }
         if (a.keep_labels)
             k_cells_walk<WALK_MINB, true><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
         else
@@ -2473,6 +2623,7 @@ void configure_cells_kernels()
     cudaFuncSetAttribute(k_cells_first<FIRST_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_walk<WALK_MINB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     cudaFuncSetAttribute(k_cells_walk<WALK_MINB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
+    cudaFuncSetAttribute(k_bucket_walk<WALK_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32);
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_cells_first<FIRST_MINB>, 32 * CELLS_WPB, sm32) ==
             cudaSuccess &&
@@ -2483,6 +2634,11 @@ void configure_cells_kernels()
             cudaSuccess &&
         nb > 0)
         g_blocks_per_smw = nb;
+    nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_bucket_walk<WALK_MINB>, 32 * CELLS_WPB, sm32) ==
+            cudaSuccess &&
+        nb > 0)
+        g_blocks_per_smb = nb;
     nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_integrate<8>, 32 * CELLS_WPB, sm32) == cudaSuccess &&
         nb > 0)

@@ -6,7 +6,7 @@
 //   buckets   int     bstart[nb+1]  CSR into the sorted sites, row-major
 //             (bucket (u,v) = u + v*bx) over the sites' bounding box
 //   tree      double4 tstat[nodes] {box centre x, y, half width, half height} (static; empty: half width -1)
-//             double4 tdyn[nodes]  {cx, cy, A, 0} plane bound (per evaluation)
+//             double4 tdyn[nodes]  {ax, ay, B, 0} weight bound (per evaluation)
 //             level 0 = the buckets, each higher level merges 2x2 nodes
 //   density   double  rho[nx*ny] density per unit area, rho[ix + iy*nx]
 //
@@ -20,6 +20,7 @@
 #define COT_MAX_HIST 32
 #define COT_BASIS (2 * COT_MAX_HIST + 1)
 #define COT_NBC 16  // cached neighbours per cell
+#define COT_BLEAF 64 // leaf buckets listed per bucket by the bucket walk (<= the frontier)
 
 // Static geometry, passed by value to the kernels.
 struct CotGeo {
@@ -36,13 +37,13 @@ struct CotGeo {
     int lev_w[COT_MAX_LEVELS];
     int lev_h[COT_MAX_LEVELS];
     const double4 *tstat;  // {box centre x, y, half width, half height}; empty: half width < 0
-    double4 *tdyn;         // {cx, cy, A, 0}
+    double4 *tdyn;         // {ax, ay, B, 0}: w_j/2 <= a.s_j + B over the node
     const double *rho;     // density per unit area
     int nx, ny;            // pixels along x, along y
     double pd[4];          // proj_domain {xmin, xmax, ymin, ymax}
     double xs, ys;         // pixel extent (reference x_step, y_step)
     double ixs, iys;       // their reciprocals
-    double margin;         // safety margin of the plane-bound exclusion test
+    double margin;         // safety margin of the bound-tree exclusion test
 };
 
 // Per-evaluation scalar results (written by the reduction's last block).
@@ -125,7 +126,7 @@ struct CellsArgs {
     const double *d;       // direction (nullable)
     const double *tptr;    // device scalar step (nullable => 0)
     double *wt;            // trial weights out
-    double *phibar;        // per bucket mean phi (scratch)
+    double *wbar;          // per bucket mean w/2 (scratch)
     double *mu;            // per cell mass out
     double *fc;            // per cell objective out, without its -w_i nu_i term
     int *nv;               // per cell ring size out
@@ -136,7 +137,7 @@ struct CellsArgs {
                            // ovf_list2 size, [4] second-pass fetch, [5]
                            // large-ring fetch over ovf_list2, [6] integration
                            // fetch, [7] unused, [8] the certificate
-                           // kernel's fetch
+                           // kernel's fetch, [9] the bucket walk's fetch
     int *nbc;              // cached neighbours, COT_NBC per cell (nullable)
     int *nbn;              // their count per cell (0: none)
     double *cen;           // centroids (nullable)
@@ -161,6 +162,11 @@ struct CellsArgs {
     int *hcnt;             // per cell: row length (ELL), or -(slot + 1) for a big row
     double *hdiag;         // per cell: dmu_i/dw_i
     int *herr;             // set when a big row found no slot
+    // the leaf buckets that can reach any ring of a bucket, rebuilt by each
+    // evaluation on the two-kernel path (nullable): COT_BLEAF per bucket in
+    // walk order, the count (-1: too many)
+    int *blist;
+    int *bcnt;
 };
 
 #define COT_HBIG_W 256  // entries of a big Jacobian row (the large-ring pass's capacity)
