@@ -31,6 +31,8 @@ namespace cot {
 
 #define FULLMASK 0xffffffffu
 #define COT_FRMAX 96
+#define COT_REFINE_PASSES 3  // ring refinements before a walk that overflows scans every bucket
+#define COT_REFINE_ROUNDS 4  // point-location rounds of one refinement
 static_assert(COT_BLEAF <= COT_FRMAX && COT_BLEAF % 32 == 0, "a bucket list fits a frontier");
 
 #ifdef COT_PHASE_STATS
@@ -1512,6 +1514,89 @@ __device__ __noinline__ RegPoly apply_chunk_cold(RegPoly P, int jl, const double
     return apply_chunk<LPC>(P, jl, sxy, si, wi, wt, lane, S, nearest);
 }
 
+// Upper bound of P_j(x) = x.s_j - phi_j over the sites of a tree node at the
+// absolute point x: F(x + a) + B, the bound node_excluded tests (-inf for an
+// empty node).
+__device__ __forceinline__ double node_upper(const CotGeo &g, int node, double x, double y)
+{
+    const double4 st = g.tstat[node];
+    if (st.z < 0.0) return -INFINITY;
+    const double4 dy = g.tdyn[node];
+    const double tx = x + dy.x, ty = y + dy.y;
+    const double ex = fmax(fabs(tx - st.x) - st.z, 0.0);
+    const double ey = fmax(fabs(ty - st.y) - st.w, 0.0);
+    return 0.5 * (__fma_rn(tx, tx, ty * ty) - __fma_rn(ex, ex, ey * ey)) + dy.z;
+}
+
+// Shrinks a ring that is far larger than its cell, for a certificate walk
+// whose frontier overflowed.  Each lane takes one vertex x of the ring and
+// descends the bound tree greedily (at every level the node with the largest
+// bound at x, at the leaf the site with the largest P_j(x)); a site that
+// beats P_i at x cuts that vertex off.  The distinct sites found are applied
+// like any other candidates, and the search repeats on the new ring, up to
+// `rounds` times or until no vertex finds a site.  Every clip is by a site
+// that cuts the ring, so the ring still contains the cell; the walk that
+// follows certifies it, and the cell's result is the one any other clip
+// order gives.
+template <int LPC>
+__device__ __noinline__ RegPoly refine_by_vertices(const CotGeo &g, const double *__restrict__ wt, int i, double2 si,
+                                                   double wi, RegPoly P, FastScratch &S, int rounds)
+{
+    const Seg<LPC> SG;
+    const int lane = SG.sl;
+    int top = g.nlev - 1;
+    while (top > 0 && g.lev_w[top - 1] * g.lev_h[top - 1] <= (LPC < 16 ? 16 : LPC)) top--;
+    const int tw = g.lev_w[top], ntop = tw * g.lev_h[top], toff = g.lev_off[top];
+    const double phi_i = 0.5 * (__fma_rn(si.x, si.x, si.y * si.y) - wi);
+    for (int r = 0; r < rounds && P.nv > 0; r++) {
+        int jl = -1;
+        if (lane < P.nv) {
+            const double x = si.x + P.x, y = si.y + P.y;
+            const double pi = __fma_rn(x, si.x, y * si.y) - phi_i;
+            int bu = -1, bv = -1;
+            double best = -INFINITY;
+            for (int q = 0; q < ntop; q++) {
+                const double ub = node_upper(g, toff + q, x, y);
+                if (ub > best) { best = ub; bu = q % tw; bv = q / tw; }
+            }
+            for (int L = top; L > 0 && bu >= 0; L--) {
+                const int cw = g.lev_w[L - 1], ch = g.lev_h[L - 1], off = g.lev_off[L - 1];
+                int nu = -1, nw = -1;
+                best = -INFINITY;
+                for (int bb = 0; bb < 2; bb++)
+                    for (int aa = 0; aa < 2; aa++) {
+                        const int cu = 2 * bu + aa, cv = 2 * bv + bb;
+                        if (cu < cw && cv < ch) {
+                            const double ub = node_upper(g, off + cu + cv * cw, x, y);
+                            if (ub > best) { best = ub; nu = cu; nw = cv; }
+                        }
+                    }
+                bu = nu;
+                bv = nw;
+            }
+            if (bu >= 0) {
+                const int b = bu + bv * g.lev_w[0];
+                double bp = pi;
+                for (int j = g.bstart[b], e = g.bstart[b + 1]; j < e; j++) {
+                    if (j == i) continue;
+                    const double2 sj = g.xy[j];
+                    const double pj = __fma_rn(x, sj.x, y * sj.y) - 0.5 * (__fma_rn(sj.x, sj.x, sj.y * sj.y) - wt[j]);
+                    if (pj > bp) { bp = pj; jl = j; }
+                }
+            }
+        }
+        // one copy of each site
+        for (int t = 0; t < LPC; t++) {
+            const int o = SG.shfl(jl, t);
+            if (t < lane && o == jl) jl = -1;
+        }
+        if (SG.ballot(jl >= 0) == 0u) break;
+        P = apply_chunk<LPC>(P, jl, g.xy, si, wi, wt, lane, S, false);
+        if (P.nv < 0) break;
+    }
+    return P;
+}
+
 // One cell, worked by one segment of LPC lanes (lane = index in the segment),
 // in three phases: cell_first (the first candidates), cell_walk (the
 // certificate over the bound tree) and cell_finish (integrals or the ring
@@ -1629,7 +1714,11 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
     const int bu = bi % g.bx, bv = bi / g.bx;
     const int win = cached ? -1 : COT_WIN;
     // ---- 2. certificate over the bound tree --------------------------------
+    // A walk whose frontier overflows means a ring far larger than its cell:
+    // the ring is shrunk by point location at its vertices and walked again
+    // (COT_REFINE_PASSES times at most) before every bucket is tested.
     bool brute = false;
+    for (int pass = 0;; pass++) {
     if (ok && P.nv > 0 && g.nlev > 0) {
         if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
         SG.sync();
@@ -1735,6 +1824,12 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
                 ok = P.nv >= 0;
             }
         }
+    }
+    if (!brute || !ok || P.nv <= 0 || pass == COT_REFINE_PASSES) break;
+    P = refine_by_vertices<LPC>(g, wt, i, si, wi, P, S, COT_REFINE_ROUNDS);
+    ok = P.nv >= 0;
+    brute = false;
+    SG.sync();
     }
     PSTAT_ADD(9, brute ? 1 : 0);
     if (ok && brute && P.nv > 0) {
@@ -1904,7 +1999,7 @@ __device__ __forceinline__ void fast_cell(const CotGeo &g, const CellsArgs &a, c
 // rings above LPC vertices into ovf_list; pass 1: the cells of ovf_list,
 // rings above LPC into ovf_list2.
 template <int MINB, bool EXACT, int LPC>
-__global__ void __launch_bounds__(128, MINB) k_cells_fast(CotGeo g, CellsArgs a, int pass)
+__global__ void __launch_bounds__(128, MINB) k_cells_fast(const __grid_constant__ CotGeo g, CellsArgs a, int pass)
 {
     static_assert(!EXACT || LPC == 32, "the exact path works a whole warp per cell");
     constexpr int CPW = 32 / LPC;
@@ -2085,7 +2180,7 @@ __global__ void __launch_bounds__(128, MINB) k_bucket_walk(CotGeo g, CellsArgs a
 // KEEP: leave the final ring's generators in lbuf (the Newton solve's
 // Jacobian reads them); a separate instance keeps the solve's path as it is.
 template <int MINB, bool KEEP>
-__global__ void __launch_bounds__(128, MINB) k_cells_walk(CotGeo g, CellsArgs a)
+__global__ void __launch_bounds__(128, MINB) k_cells_walk(const __grid_constant__ CotGeo g, CellsArgs a)
 {
     constexpr int LPC = 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
