@@ -26,6 +26,7 @@
 #include "cot_edge.cuh"
 #include <math.h>
 #include <algorithm>
+#include <climits>
 
 namespace cot {
 
@@ -59,6 +60,8 @@ __shared__ unsigned long long cot_pst[16][16];
 // cell at the last evaluation
 #define COT_NB_HIDDEN 100
 #define COT_RCAP 32  // ring buffer vertices per cell (the split integration)
+#define COT_HEAVY_PIX 1024  // pixel box above which a cell is integrated first
+#define CST_HEAVY (-2)      // cstate of a cell on the heavy integration list
 
 // ---------------------------------------------------------------------------
 // bucket and tree weight bounds (per evaluation)
@@ -1909,6 +1912,23 @@ __device__ __forceinline__ void cell_finish(const CotGeo &g, const CellsArgs &a,
             acc = integrate_cell(S, nv, splat_geo(g, a, S, nv, i, lane), si, lane);
         else if (lane < nv)
             a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.x, P.y);
+        if constexpr (!EXACT && LPC == 32) {
+            // a cell whose pixel box is large goes on the heavy list: the
+            // integration kernel starts those cells first, so that they run
+            // beside the many small ones instead of after them
+            if (a.hlist != nullptr) {
+                const double ox = si.x - g.pd[0], oy = si.y - g.pd[2];
+                const int cx = lane < nv ? (int)floor((ox + P.x) * g.ixs) : INT_MAX;
+                const int cy = lane < nv ? (int)floor((oy + P.y) * g.iys) : INT_MAX;
+                const int c0 = __reduce_min_sync(FULLMASK, cx), r0 = __reduce_min_sync(FULLMASK, cy);
+                const int c1 = __reduce_max_sync(FULLMASK, lane < nv ? cx : INT_MIN);
+                const int r1 = __reduce_max_sync(FULLMASK, lane < nv ? cy : INT_MIN);
+                if ((double)(c1 - c0 + 1) * (double)(r1 - r0 + 1) > (double)COT_HEAVY_PIX && lane == 0) {
+                    a.hlist[atomicAdd(a.ovf_count + 10, 1)] = i;
+                    a.cstate[i] = CST_HEAVY;
+                }
+            }
+        }
         // the Newton solve's Jacobian reads the final ring's generators
         if constexpr (KEEP) {
             if (lane < nv) a.lbuf[(size_t)i * COT_RCAP + lane] = P.l;
@@ -2234,11 +2254,20 @@ __global__ void __launch_bounds__(128, MINB) k_integrate(CotGeo g, CellsArgs a)
     FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     int *fetch = a.ovf_count + 6;
+    // the heavy list first, then every other cell in order
+    const int nh = a.hlist != nullptr ? a.ovf_count[10] : 0;
     while (true) {
-        int i = 0;
-        if (lane == 0) i = atomicAdd(fetch, 1);
-        i = __shfl_sync(FULLMASK, i, 0);
-        if (i >= g.n) break;
+        int f = 0;
+        if (lane == 0) f = atomicAdd(fetch, 1);
+        f = __shfl_sync(FULLMASK, f, 0);
+        if (f >= g.n + nh) break;
+        int i;
+        if (f < nh) {
+            i = a.hlist[f];
+        } else {
+            i = f - nh;
+            if (nh > 0 && a.cstate[i] == CST_HEAVY) continue;
+        }
         const int nv = a.nv[i];
         if (nv > COT_RCAP) continue;
         double mu = 0.0, fcv = 0.0;
@@ -2613,9 +2642,9 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
     while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
     // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
     // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter,
-    // [9]: k_bucket_walk's
+    // [9]: k_bucket_walk's, [10]: the heavy integration list's size
     const int segs = (nb * BSEG + 127) / 128;
-    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 10);
+    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 12);
     k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.wbar);
     c.launches += 2;
     int upper = 0;  // nodes of levels 1..lmax
@@ -2630,6 +2659,9 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
     // the bucket walk's lists exist only on the path that runs it: every
     // other path walks in full
     if (exact || lpc != 32) a.blist = a.bcnt = nullptr;
+    // the heavy integration list (ovf_list2, which only the 16- and 8-lane
+    // paths use otherwise) on the two-kernel path
+    a.hlist = (exact || lpc != 32) ? nullptr : a.ovf_list2;
     const int per_sm32 = g_blocks_per_sm32 > 0 ? g_blocks_per_sm32 : CELLS_MINB;
     const int per_sm16 = g_blocks_per_sm16 > 0 ? g_blocks_per_sm16 : CELLS_MINB;
     const int per_sm8 = g_blocks_per_sm8 > 0 ? g_blocks_per_sm8 : 1;

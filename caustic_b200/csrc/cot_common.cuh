@@ -167,6 +167,10 @@ struct CellsArgs {
     // walk order, the count (-1: too many)
     int *blist;
     int *bcnt;
+    // cells whose integration covers a large pixel box, listed by the
+    // certificate kernel so that the integration kernel starts them first
+    // (two-kernel path only; nullable)
+    int *hlist;
 };
 
 #define COT_HBIG_W 256  // entries of a big Jacobian row (the large-ring pass's capacity)
