@@ -50,6 +50,7 @@ struct CotProblemDev {
     int *lbuf = nullptr;      // ring generators between the two ring-building kernels
     int *cstate = nullptr;    // per-cell state between them
     int *nv = nullptr, *ovf_list = nullptr, *ovf_list2 = nullptr, *ovf_count = nullptr;
+    int *wlist = nullptr;  // cells whose certificate walk overflowed (finished a block each)
     int *nbc = nullptr, *nbn = nullptr;        // neighbour cache of the solves
     int *nbc_q = nullptr, *nbn_q = nullptr;    // and of the query entry points
     double *partials = nullptr;
@@ -171,7 +172,7 @@ using namespace cot;
 static void free_sized_by_sites(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.sbucket, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut, P.wq, P.fc, P.rbuf, P.lbuf,
-                    P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials,
+                    P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.wlist, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials,
                     P.ticket, P.out, P.tmp, P.S, P.Sv, P.Yv, P.hval, P.hdiag, P.hbig_val, P.hcol, P.hcnt,
                     P.hbig_col, P.herr, P.nb_b, P.nb_r, P.nb_z, P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.nb_tau, P.pcg,
                     P.nst, P.nticket, P.bpart, P.bticket, P.bstat, P.cubtmp};
@@ -179,7 +180,7 @@ static void free_sized_by_sites(CotProblemDev &P)
         if (p) cudaFree(p);
     P.xy = nullptr; P.nu = nullptr; P.sbucket = nullptr; P.rho = nullptr; P.perm = nullptr;
     P.w = P.wt = P.d = P.mu = P.mut = P.wq = P.fc = nullptr;
-    P.rbuf = nullptr; P.lbuf = P.cstate = P.nv = P.ovf_list = P.ovf_list2 = P.ovf_count = nullptr;
+    P.rbuf = nullptr; P.lbuf = P.cstate = P.nv = P.ovf_list = P.ovf_list2 = P.ovf_count = P.wlist = nullptr;
     P.nbc = P.nbn = P.nbc_q = P.nbn_q = nullptr;
     P.partials = nullptr; P.ticket = nullptr; P.out = nullptr; P.tmp = nullptr; P.S = nullptr;
     P.Sv = P.Yv = nullptr; P.hist_alloc = 0;
@@ -381,6 +382,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const double *xy_in, c
         A((void **)&P.ovf_list, N * sizeof(int));
         A((void **)&P.ovf_list2, N * sizeof(int));
         A((void **)&P.ovf_count, 16 * sizeof(int));
+        A((void **)&P.wlist, N * sizeof(int));
         A((void **)&P.nbc, N * COT_NBC * sizeof(int));
         A((void **)&P.nbn, N * sizeof(int));
         A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
@@ -610,6 +612,7 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.ovf_list = P.ovf_list;
     a.ovf_list2 = P.ovf_list2;
     a.ovf_count = P.ovf_count;
+    a.wlist = P.wlist;
     // the query entry points (weights in P.wq) keep their own neighbour cache
     // so that a query made during a solve does not change the solve's clip
     // order

@@ -34,6 +34,7 @@ namespace cot {
 #define COT_FRMAX 96
 #define COT_REFINE_PASSES 3  // ring refinements before a walk that overflows scans every bucket
 #define COT_REFINE_ROUNDS 4  // point-location rounds of one refinement
+#define COT_DEFERRED (-3)    // ring size of a cell handed to k_cells_heavy
 static_assert(COT_BLEAF <= COT_FRMAX && COT_BLEAF % 32 == 0, "a bucket list fits a frontier");
 
 #ifdef COT_PHASE_STATS
@@ -1600,6 +1601,39 @@ __device__ __noinline__ RegPoly refine_by_vertices(const CotGeo &g, const double
     return P;
 }
 
+// Every bucket tested against the current ring, and the sites of those
+// that can cut it applied (the buckets of the window around (bu, bv) are
+// skipped: their sites were applied already).  The last resort of a
+// certificate whose frontier overflows.
+template <int LPC>
+__device__ __noinline__ RegPoly scan_all_buckets(const CotGeo &g, const double *__restrict__ wt, int i, double2 si,
+                                                 double wi, RegPoly P, FastScratch &S, int bu, int bv, int win)
+{
+    const Seg<LPC> SG;
+    const int lane = SG.sl;
+    const int nb = g.bx * g.by;
+    for (int base = 0; base < nb && P.nv > 0; base += LPC) {
+        if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
+        SG.sync();
+        const int b = base + lane;
+        bool keep = false;
+        if (b < nb) {
+            const int u = b % g.bx, v = b / g.bx;
+            const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
+            keep = !inwin && !node_excluded(S, P.nv, g, b, si, wi);
+        }
+        SG.sync();
+        int st = 0, cnt = 0;
+        if (keep) {
+            st = g.bstart[b];
+            cnt = g.bstart[b + 1] - st;
+        }
+        const int inc = SG.incl_scan(cnt);
+        P = apply_ranges<LPC>(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
+    }
+    return P;
+}
+
 // One cell, worked by one segment of LPC lanes (lane = index in the segment),
 // in three phases: cell_first (the first candidates), cell_walk (the
 // certificate over the bound tree) and cell_finish (integrals or the ring
@@ -1828,37 +1862,33 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
             }
         }
     }
-    if (!brute || !ok || P.nv <= 0 || pass == COT_REFINE_PASSES) break;
+    if (!brute || !ok || P.nv <= 0) break;
+    if (pass == COT_REFINE_PASSES) {
+        if constexpr (LPC == 32) {
+            // on the two-kernel path the refined ring goes to the ring
+            // buffer and k_cells_heavy finishes the cell with a block
+            if (a.wlist != nullptr) {
+                if (lane < P.nv) {
+                    a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.x, P.y);
+                    a.lbuf[(size_t)i * COT_RCAP + lane] = P.l;
+                }
+                if (lane == 0) {
+                    a.cstate[i] = P.nv;
+                    a.wlist[atomicAdd(a.ovf_count + 11, 1)] = i;
+                }
+                P.nv = COT_DEFERRED;
+                return P;
+            }
+        }
+        break;
+    }
     P = refine_by_vertices<LPC>(g, wt, i, si, wi, P, S, COT_REFINE_ROUNDS);
     ok = P.nv >= 0;
     brute = false;
     SG.sync();
     }
     PSTAT_ADD(9, brute ? 1 : 0);
-    if (ok && brute && P.nv > 0) {
-        // frontier overflow: test every bucket against the current ring
-        const int nb = g.bx * g.by;
-        for (int base = 0; base < nb && ok && P.nv > 0; base += LPC) {
-            if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; }
-            SG.sync();
-            const int b = base + lane;
-            bool keep = false;
-            if (b < nb) {
-                const int u = b % g.bx, v = b / g.bx;
-                const bool inwin = abs(u - bu) <= win && abs(v - bv) <= win;
-                keep = !inwin && !node_excluded(S, P.nv, g, b, si, wi);
-            }
-            SG.sync();
-            int st = 0, cnt = 0;
-            if (keep) {
-                st = g.bstart[b];
-                cnt = g.bstart[b + 1] - st;
-            }
-            const int inc = SG.incl_scan(cnt);
-            P = apply_ranges_cold<LPC>(P, st, cnt, inc, i, g.xy, si, wi, wt, lane, S, false);
-            ok = P.nv >= 0;
-        }
-    }
+    if (ok && brute && P.nv > 0) P = scan_all_buckets<LPC>(g, wt, i, si, wi, P, S, bu, bv, win);
     PSTAT_CLOCK(t2);
     PSTAT_ADD(1, t2 - t1);
     return P;
@@ -2237,10 +2267,254 @@ __global__ void __launch_bounds__(128, MINB) k_cells_walk(const __grid_constant_
         if (lane == 0) S.kn = -1;
         __syncwarp();
         P = cell_walk<LPC>(g, a, i, si, wi, P, (st & CST_CACHED) != 0, S);
-        cell_finish<false, LPC, KEEP>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
+        if (P.nv != COT_DEFERRED) cell_finish<false, LPC, KEEP>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
         __syncwarp();
     }
     PSTAT_FLUSH();
+}
+
+// The cells whose certificate walk still overflowed its frontier after the
+// ring refinements (listed by k_cells_walk, the refined ring in the ring
+// buffer), one block of HEAVY_WARPS warps a cell.  Every warp tests its share
+// of the buckets against the ring, then the sites of the buckets that can cut
+// it, lanes over sites, and lists the sites that cut with their depth (how
+// far the ring reaches past the site's line).  Then, round by round, warp 0
+// applies the 32 deepest listed sites, deepest first, and the warps drop the
+// listed sites that no longer cut the smaller ring.  A site that cuts the
+// final ring cuts every ring that contains it, so none is missed, and the
+// cell is the one any other clip order gives; the order is fixed (depth, then
+// index), so a run repeats bit for bit.  Lists that outgrow their room are
+// cut short: the rounds run on what was found, and the search starts again
+// (HEAVY_RETRY times, then warp 0 scans every bucket).
+#define HEAVY_WARPS 8
+#define HEAVY_KCAP 256  // buckets that can cut, per warp
+#define HEAVY_CCAP 512  // sites that cut, per warp
+#define HEAVY_RETRY 4
+struct HeavyShared {
+    int kept[HEAVY_WARPS][HEAVY_KCAP];
+    int cut[HEAVY_WARPS][HEAVY_CCAP];
+    float dep[HEAVY_WARPS][HEAVY_CCAP];
+    float tdep[HEAVY_WARPS][32];
+    int tj[HEAVY_WARPS][32];
+    int ncut[HEAVY_WARPS], over[HEAVY_WARPS];
+    int cell, nv;
+};
+static_assert(sizeof(FastScratch) + sizeof(HeavyShared) <= 48 * 1024, "k_cells_heavy fits the default shared memory");
+
+// Depth of site j's cut into the ring snapshot (S.X, S.Y, S.L, nv vertices):
+// the largest distance of a vertex past the site's line, or -1 when the site
+// does not cut (apply_chunk's test).
+__device__ __forceinline__ float site_depth(const CotGeo &g, const double *__restrict__ wt, int j, double2 si,
+                                            double wi, const FastScratch &S, int nv)
+{
+    double al, bl, cl, key;
+    site_line(g.xy[j], si, wt[j], wi, al, bl, cl, key);
+    double dm = 0.0;
+    for (int q = 0; q < nv; q++) {
+        if (S.L[q] == j) return -1.0f;
+        dm = fmax(dm, side(al, bl, cl, S.X[q], S.Y[q]));
+    }
+    if (!(dm > 0.0)) return -1.0f;
+    return (float)(dm / sqrt(key));
+}
+
+// (depth, index) order: deeper first, then the lower index.
+__device__ __forceinline__ bool deeper(float d1, int j1, float d2, int j2)
+{
+    return d1 > d2 || (d1 == d2 && j1 < j2);
+}
+
+// Bitonic step helpers over a warp holding one (depth, index) pair a lane.
+__device__ __forceinline__ void cmpx(float &d, int &j, int mask, bool keep_deeper)
+{
+    const float od = __shfl_xor_sync(FULLMASK, d, mask);
+    const int oj = __shfl_xor_sync(FULLMASK, j, mask);
+    const bool od_first = deeper(od, oj, d, j);
+    if (od_first == keep_deeper) { d = od; j = oj; }
+}
+
+// Sorts the warp's pairs, deepest at lane 0.
+__device__ __forceinline__ void warp_sort_deep(float &d, int &j, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int m = k >> 1; m > 0; m >>= 1) {
+            const bool lower = (lane & m) == 0;
+            const bool asc = (lane & k) == 0;  // this run sorts deepest first
+            cmpx(d, j, m, lower == asc);
+        }
+}
+
+// top (sorted, deepest at lane 0) := the 32 deepest of top and the sorted c.
+__device__ __forceinline__ void warp_merge_top(float &td, int &tj, float cd, int cj, int lane)
+{
+    // c reversed against top is a bitonic sequence; the lane-wise deeper half
+    // holds the 32 deepest, sorted again by a bitonic clean-up
+    const float rd = __shfl_sync(FULLMASK, cd, 31 - lane);
+    const int rj = __shfl_sync(FULLMASK, cj, 31 - lane);
+    if (deeper(rd, rj, td, tj)) { td = rd; tj = rj; }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) cmpx(td, tj, m, (lane & m) == 0);
+}
+
+template <bool KEEP>
+__global__ void __launch_bounds__(32 * HEAVY_WARPS, 2) k_cells_heavy(const __grid_constant__ CotGeo g, CellsArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FastScratch &S = *reinterpret_cast<FastScratch *>(smem_raw);
+    HeavyShared &H = *reinterpret_cast<HeavyShared *>(smem_raw + sizeof(FastScratch));
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int total = a.ovf_count[11];
+    const int nb = g.bx * g.by;
+    while (true) {
+        if (threadIdx.x == 0) H.cell = atomicAdd(a.ovf_count + 12, 1);
+        __syncthreads();
+        const int f = H.cell;
+        if (f >= total) break;
+        const int i = a.wlist[f];
+        const double2 si = g.xy[i];
+        const double wi = a.wt[i];
+        RegPoly P;
+        if (wp == 0) {
+            P.nv = a.cstate[i] & 0xff;
+            P.x = P.y = P.a = P.b = P.c = 0.0;
+            P.l = 0;
+            if (lane < P.nv) {
+                const double2 v = a.rbuf[(size_t)i * COT_RCAP + lane];
+                P.x = v.x;
+                P.y = v.y;
+                P.l = a.lbuf[(size_t)i * COT_RCAP + lane];
+                if (P.l >= 0) {
+                    double key;
+                    site_line(g.xy[P.l], si, a.wt[P.l], wi, P.a, P.b, P.c, key);
+                } else {
+                    const double4 box = make_double4(g.pd[0] - si.x, g.pd[1] - si.x, g.pd[2] - si.y, g.pd[3] - si.y);
+                    side_line(-P.l - 1, box, P.a, P.b, P.c);
+                }
+                S.X[lane] = P.x;
+                S.Y[lane] = P.y;
+                S.L[lane] = P.l;
+            }
+            if (lane == 0) {
+                S.kn = -1;
+                H.nv = P.nv;
+            }
+        }
+        __syncthreads();
+        bool over = false;
+        for (int attempt = 0;; attempt++) {
+            // the sites that cut the ring, per warp in a fixed order, with the
+            // warp's 32 deepest
+            int nv = H.nv;
+            if (nv > 0) {
+                int nk = 0, nc = 0;
+                bool ov = false;
+                for (int base = wp * 32; base < nb; base += 32 * HEAVY_WARPS) {
+                    const int b = base + lane;
+                    const bool keep = b < nb && !node_excluded(S, nv, g, b, si, wi);
+                    const unsigned m = __ballot_sync(FULLMASK, keep);
+                    if (nk + __popc(m) > HEAVY_KCAP) { ov = true; break; }
+                    if (keep) H.kept[wp][nk + __popc(m & lt)] = b;
+                    nk += __popc(m);
+                }
+                __syncwarp();
+                float td = -1.0f;
+                int tj = INT_MAX;
+                for (int k = 0; k < nk; k++) {
+                    const int b = H.kept[wp][k];
+                    const int s1 = g.bstart[b + 1];
+                    bool full = false;
+                    for (int j0 = g.bstart[b]; j0 < s1; j0 += 32) {
+                        const int j = j0 + lane;
+                        const float dj = (j < s1 && j != i) ? site_depth(g, a.wt, j, si, wi, S, nv) : -1.0f;
+                        const bool cut = dj > 0.0f;
+                        const unsigned m = __ballot_sync(FULLMASK, cut);
+                        if (nc + __popc(m) > HEAVY_CCAP) { full = true; break; }
+                        if (cut) {
+                            H.cut[wp][nc + __popc(m & lt)] = j;
+                            H.dep[wp][nc + __popc(m & lt)] = dj;
+                        }
+                        nc += __popc(m);
+                        if (m != 0u) {
+                            float cd = cut ? dj : -1.0f;
+                            int cj = cut ? j : INT_MAX;
+                            warp_sort_deep(cd, cj, lane);
+                            warp_merge_top(td, tj, cd, cj, lane);
+                        }
+                    }
+                    if (full) { ov = true; break; }
+                }
+                H.tdep[wp][lane] = td;
+                H.tj[wp][lane] = tj;
+                if (lane == 0) {
+                    H.ncut[wp] = nc;
+                    H.over[wp] = ov ? 1 : 0;
+                }
+            }
+            __syncthreads();
+            over = false;
+            for (int q = 0; q < HEAVY_WARPS; q++) over = over || (nv > 0 && H.over[q] != 0);
+            // rounds: the 32 deepest first; then drop what no longer cuts
+            while (nv > 0) {
+                if (wp == 0) {
+                    float td = H.tdep[0][lane];
+                    int tj = H.tj[0][lane];
+                    for (int q = 1; q < HEAVY_WARPS; q++) warp_merge_top(td, tj, H.tdep[q][lane], H.tj[q][lane], lane);
+                    const int jl = td > 0.0f ? tj : -1;
+                    if (__ballot_sync(FULLMASK, jl >= 0) != 0u) {
+                        P = apply_chunk<32>(P, jl, g.xy, si, wi, a.wt, lane, S, false);
+                        if (lane < P.nv) { S.X[lane] = P.x; S.Y[lane] = P.y; S.L[lane] = P.l; }
+                        if (lane == 0) H.nv = P.nv;
+                    } else if (lane == 0) {
+                        H.nv = -100 - P.nv;  // nothing left to apply (decoded below)
+                    }
+                }
+                __syncthreads();
+                nv = H.nv;
+                if (nv <= -100) {
+                    nv = -100 - nv;
+                    __syncthreads();
+                    if (threadIdx.x == 0) H.nv = nv;
+                    __syncthreads();
+                    break;
+                }
+                if (nv <= 0) break;
+                const int n0 = H.ncut[wp];
+                int nk = 0;
+                float td = -1.0f;
+                int tj = INT_MAX;
+                for (int base = 0; base < n0; base += 32) {
+                    const int k = base + lane;
+                    const int j = k < n0 ? H.cut[wp][k] : -1;
+                    const float dj = j >= 0 ? site_depth(g, a.wt, j, si, wi, S, nv) : -1.0f;
+                    const bool cut = dj > 0.0f;
+                    const unsigned m = __ballot_sync(FULLMASK, cut);
+                    if (cut) {
+                        H.cut[wp][nk + __popc(m & lt)] = j;
+                        H.dep[wp][nk + __popc(m & lt)] = dj;
+                    }
+                    nk += __popc(m);
+                    if (m != 0u) {
+                        float cd = cut ? dj : -1.0f;
+                        int cj = cut ? j : INT_MAX;
+                        warp_sort_deep(cd, cj, lane);
+                        warp_merge_top(td, tj, cd, cj, lane);
+                    }
+                    __syncwarp();
+                }
+                H.tdep[wp][lane] = td;
+                H.tj[wp][lane] = tj;
+                if (lane == 0) H.ncut[wp] = nk;
+                __syncthreads();
+            }
+            if (nv <= 0 || !over || attempt == HEAVY_RETRY) break;
+        }
+        if (H.nv > 0 && over && wp == 0) P = scan_all_buckets<32>(g, a.wt, i, si, wi, P, S, 0, 0, -1);
+        if (wp == 0) cell_finish<false, 32, KEEP>(g, a, i, si, wi, P, S, a.ovf_list, a.ovf_count);
+        __syncthreads();
+    }
 }
 
 // The masses and objective terms of the cells whose rings k_cells_fast left
@@ -2642,9 +2916,10 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
     while (lmax < g.nlev - 1 && g.lev_w[lmax] * g.lev_h[lmax] > 16) lmax++;
     // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
     // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter,
-    // [9]: k_bucket_walk's, [10]: the heavy integration list's size
+    // [9]: k_bucket_walk's, [10]: the heavy integration list's size, [11]:
+    // the overflowed walks' list size, [12]: k_cells_heavy's fetch counter
     const int segs = (nb * BSEG + 127) / 128;
-    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 12);
+    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 13);
     k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.wbar);
     c.launches += 2;
     int upper = 0;  // nodes of levels 1..lmax
@@ -2662,6 +2937,7 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
     // the heavy integration list (ovf_list2, which only the 16- and 8-lane
     // paths use otherwise) on the two-kernel path
     a.hlist = (exact || lpc != 32) ? nullptr : a.ovf_list2;
+    if (exact || lpc != 32) a.wlist = nullptr;
     const int per_sm32 = g_blocks_per_sm32 > 0 ? g_blocks_per_sm32 : CELLS_MINB;
     const int per_sm16 = g_blocks_per_sm16 > 0 ? g_blocks_per_sm16 : CELLS_MINB;
     const int per_sm8 = g_blocks_per_sm8 > 0 ? g_blocks_per_sm8 : 1;
@@ -2686,6 +2962,14 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
             k_cells_walk<WALK_MINB, true><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
         else
             k_cells_walk<WALK_MINB, false><<<(bw + CELLS_WPB - 1) / CELLS_WPB, 32 * CELLS_WPB, sm, s>>>(g, a);
+        c.launches++;
+        // the cells whose walk overflowed, a block each (an empty list
+        // returns at once)
+        const size_t hsm = sizeof(FastScratch) + sizeof(HeavyShared);
+        if (a.keep_labels)
+            k_cells_heavy<true><<<2 * sms, 32 * HEAVY_WARPS, hsm, s>>>(g, a);
+        else
+            k_cells_heavy<false><<<2 * sms, 32 * HEAVY_WARPS, hsm, s>>>(g, a);
         c.launches++;
     } else if (lpc == 16) {
         launch_fast<false, 16>(g, a, 0, blocks, s);

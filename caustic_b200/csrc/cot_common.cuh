@@ -171,6 +171,9 @@ struct CellsArgs {
     // certificate kernel so that the integration kernel starts them first
     // (two-kernel path only; nullable)
     int *hlist;
+    // cells whose certificate walk overflowed its frontier, finished by
+    // k_cells_heavy a block each (two-kernel path only; nullable)
+    int *wlist;
 };
 
 #define COT_HBIG_W 256  // entries of a big Jacobian row (the large-ring pass's capacity)
