@@ -35,6 +35,9 @@ namespace cot {
 #define COT_REFINE_PASSES 3  // ring refinements before a walk that overflows scans every bucket
 #define COT_REFINE_ROUNDS 4  // point-location rounds of one refinement
 #define COT_DEFERRED (-3)    // ring size of a cell handed to k_cells_heavy
+#ifndef COT_DEFER_PASS
+#define COT_DEFER_PASS 1  // refinement passes before a walk is handed to k_cells_heavy (1, 2, 3 measured 134.9, 134.8, 134.3 M cell-evals/s: 65,536 sites, 1024² target)
+#endif
 static_assert(COT_BLEAF <= COT_FRMAX && COT_BLEAF % 32 == 0, "a bucket list fits a frontier");
 
 #ifdef COT_PHASE_STATS
@@ -1863,7 +1866,7 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
         }
     }
     if (!brute || !ok || P.nv <= 0) break;
-    if (pass == COT_REFINE_PASSES) {
+    if (pass == COT_DEFER_PASS || pass == COT_REFINE_PASSES) {
         if constexpr (LPC == 32) {
             // on the two-kernel path the refined ring goes to the ring
             // buffer and k_cells_heavy finishes the cell with a block
@@ -1880,7 +1883,7 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
                 return P;
             }
         }
-        break;
+        if (pass == COT_REFINE_PASSES) break;
     }
     P = refine_by_vertices<LPC>(g, wt, i, si, wi, P, S, COT_REFINE_ROUNDS);
     ok = P.nv >= 0;
