@@ -51,6 +51,9 @@ struct CotProblemDev {
     int *cstate = nullptr;    // per-cell state between them
     int *nv = nullptr, *ovf_list = nullptr, *ovf_list2 = nullptr, *ovf_count = nullptr;
     int *wlist = nullptr;  // cells whose certificate walk overflowed (finished a block each)
+    int *hsplit = nullptr;           // cells whose integration is shared by several warps
+    double *hpart = nullptr;         // their parts' raw sums
+    unsigned int *hticket = nullptr; // a ticket per slot, 0 between evaluations
     int *nbc = nullptr, *nbn = nullptr;        // neighbour cache of the solves
     int *nbc_q = nullptr, *nbn_q = nullptr;    // and of the query entry points
     double *partials = nullptr;
@@ -172,7 +175,7 @@ using namespace cot;
 static void free_sized_by_sites(CotProblemDev &P)
 {
     void *ptrs[] = {P.xy, P.nu, P.sbucket, P.rho, P.perm, P.w, P.wt, P.d, P.mu, P.mut, P.wq, P.fc, P.rbuf, P.lbuf,
-                    P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.wlist, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials,
+                    P.cstate, P.nv, P.ovf_list, P.ovf_list2, P.ovf_count, P.wlist, P.hsplit, P.hpart, P.hticket, P.nbc, P.nbn, P.nbc_q, P.nbn_q, P.partials,
                     P.ticket, P.out, P.tmp, P.S, P.Sv, P.Yv, P.hval, P.hdiag, P.hbig_val, P.hcol, P.hcnt,
                     P.hbig_col, P.herr, P.nb_b, P.nb_r, P.nb_z, P.nb_pa, P.nb_pb, P.nb_q, P.nb_part, P.nb_tau, P.pcg,
                     P.nst, P.nticket, P.bpart, P.bticket, P.bstat, P.cubtmp};
@@ -181,6 +184,7 @@ static void free_sized_by_sites(CotProblemDev &P)
     P.xy = nullptr; P.nu = nullptr; P.sbucket = nullptr; P.rho = nullptr; P.perm = nullptr;
     P.w = P.wt = P.d = P.mu = P.mut = P.wq = P.fc = nullptr;
     P.rbuf = nullptr; P.lbuf = P.cstate = P.nv = P.ovf_list = P.ovf_list2 = P.ovf_count = P.wlist = nullptr;
+    P.hsplit = nullptr; P.hpart = nullptr; P.hticket = nullptr;
     P.nbc = P.nbn = P.nbc_q = P.nbn_q = nullptr;
     P.partials = nullptr; P.ticket = nullptr; P.out = nullptr; P.tmp = nullptr; P.S = nullptr;
     P.Sv = P.Yv = nullptr; P.hist_alloc = 0;
@@ -383,6 +387,9 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const double *xy_in, c
         A((void **)&P.ovf_list2, N * sizeof(int));
         A((void **)&P.ovf_count, 16 * sizeof(int));
         A((void **)&P.wlist, N * sizeof(int));
+        A((void **)&P.hsplit, COT_HSPLIT_CAP * sizeof(int));
+        A((void **)&P.hpart, (size_t)COT_HSPLIT_CAP * COT_SPLIT * 4 * sizeof(double));
+        A((void **)&P.hticket, COT_HSPLIT_CAP * sizeof(unsigned int));
         A((void **)&P.nbc, N * COT_NBC * sizeof(int));
         A((void **)&P.nbn, N * sizeof(int));
         A((void **)&P.nbc_q, N * COT_NBC * sizeof(int));
@@ -396,6 +403,7 @@ static int build_problem(cot_handle *h, CotProblemDev &P, const double *xy_in, c
         A((void **)&P.bticket, 2 * sizeof(unsigned int));
         A((void **)&P.bstat, 256);
         if (e == cudaSuccess) e = cudaMemsetAsync(P.bticket, 0, 2 * sizeof(unsigned int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(P.hticket, 0, COT_HSPLIT_CAP * sizeof(unsigned int), s);
         if (e != cudaSuccess) {
             free_sized_by_sites(P);
             return fail(h, COT_ENOMEM, "cot_set_problem: device allocation", cudaGetErrorString(e));
@@ -613,6 +621,10 @@ static CellsArgs cells_args(CotProblemDev &P, const double *w, const double *d, 
     a.ovf_list2 = P.ovf_list2;
     a.ovf_count = P.ovf_count;
     a.wlist = P.wlist;
+    a.hsplit = P.hsplit;
+    a.hpart = P.hpart;
+    a.hticket = P.hticket;
+    a.hsplit_cap = COT_HSPLIT_CAP;
     // the query entry points (weights in P.wq) keep their own neighbour cache
     // so that a query made during a solve does not change the solve's clip
     // order

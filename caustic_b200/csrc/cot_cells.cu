@@ -65,6 +65,7 @@ __shared__ unsigned long long cot_pst[16][16];
 #define COT_NB_HIDDEN 100
 #define COT_RCAP 32  // ring buffer vertices per cell (the split integration)
 #define COT_HEAVY_PIX 1024  // pixel box above which a cell is integrated first
+#define COT_SPLIT_PIX 8192  // pixel box above which a cell is integrated by COT_SPLIT warps
 #define CST_HEAVY (-2)      // cstate of a cell on the heavy integration list
 
 // ---------------------------------------------------------------------------
@@ -889,8 +890,14 @@ __device__ __forceinline__ double line_t(double X, double p, double inv) { retur
 // (vertical line, pixel row) segment inside the cell, likewise handed out
 // by a scan over the lines.  One lane per edge: rings of up to LPC = 32
 // vertices.
-template <int LPC, class SP>
-__device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, double2 si, int lane)
+//
+// SPLIT: one part of a cell shared by `nparts` warps (the cells with very
+// large pixel boxes): part 0 takes the edge pieces, and part p the vertical
+// lines lx + p + nparts q; the part's raw sums {A, Ia, Ib, I2} and the box
+// origin go to raw[0..5] (every lane), and the caller adds the parts.
+template <int LPC, class SP, bool SPLIT = false>
+__device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g, double2 si, int lane,
+                                                  int part = 0, int nparts = 1, double *raw = nullptr)
 {
     static_assert(LPC == 32, "one lane per edge of a ring of up to 32 vertices");
     const Seg<LPC> W;
@@ -917,7 +924,7 @@ __device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g,
     // edge `lane`: first x line beyond p and count of x lines strictly
     // between p and q (cf, nxc), the same for y (rf, nyc)
     int cf = 0, nxc = 0, rf = 0, nyc = 0, cnt = 0;
-    {
+    if (!SPLIT || part == 0) {
         const double dx = qx - px, dy = qy - py;
         bool skip = !act || dy == 0.0;  // horizontal: no x-dy term
         if (!skip && dx == 0.0) {
@@ -1061,8 +1068,9 @@ __device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g,
     ly = max(ly, 0);
     hx = min(hx, g.nx);
     hy = min(hy, g.ny);
-    for (int cxs = lx; cxs <= hx; cxs += LPC) {
-        const int l = cxs + lane;
+    const int lstep = SPLIT ? nparts : 1;
+    for (int cxs = lx + (SPLIT ? part : 0); cxs <= hx; cxs += LPC * lstep) {
+        const int l = cxs + lane * lstep;
         double lo = INFINITY, hi = -INFINITY, xl = 0.0;
         int r0 = 0, rc = 0;
         bool fl = false, fr = false;
@@ -1097,7 +1105,7 @@ __device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g,
             const int r = kr0 + (t - (ik - ck));
             const double b0 = fmax(klo, lpos(r, g.ys, cy0)), b1 = fmin(khi, lpos(r + 1, g.ys, cy0));
             if (!(b1 > b0)) continue;
-            const int lk = cxs + k;
+            const int lk = cxs + k * lstep;
             const double wl = kfl ? g.rho[(lk - 1) + r * g.nx] : 0.0;
             const double wr = kfr ? g.rho[lk + r * g.nx] : 0.0;
             Mom mm = {0.0, 0.0, 0.0, 0.0};
@@ -1113,6 +1121,15 @@ __device__ __forceinline__ CellAcc integrate_fast(SP &P, int nv, const PixGeo g,
     sIa = W.sum(sIa);
     sIb = W.sum(sIb);
     sI2 = W.sum(sI2);
+    if constexpr (SPLIT) {
+        raw[0] = sA;
+        raw[1] = sIa;
+        raw[2] = sIb;
+        raw[3] = sI2;
+        raw[4] = ox;
+        raw[5] = oy;
+        return acc;
+    }
     acc.mu = sA;
     // int |x - s_i|^2 = int |(x - o) + o|^2 in the site frame
     acc.S = sI2 + 2.0 * (ox * sIa + oy * sIb) + (ox * ox + oy * oy) * sA;
@@ -1956,8 +1973,14 @@ __device__ __forceinline__ void cell_finish(const CotGeo &g, const CellsArgs &a,
                 const int c0 = __reduce_min_sync(FULLMASK, cx), r0 = __reduce_min_sync(FULLMASK, cy);
                 const int c1 = __reduce_max_sync(FULLMASK, lane < nv ? cx : INT_MIN);
                 const int r1 = __reduce_max_sync(FULLMASK, lane < nv ? cy : INT_MIN);
-                if ((double)(c1 - c0 + 1) * (double)(r1 - r0 + 1) > (double)COT_HEAVY_PIX && lane == 0) {
-                    a.hlist[atomicAdd(a.ovf_count + 10, 1)] = i;
+                const double box = (double)(c1 - c0 + 1) * (double)(r1 - r0 + 1);
+                if (box > (double)COT_HEAVY_PIX && lane == 0) {
+                    // the largest boxes are shared by COT_SPLIT warps (while
+                    // the split list has room), the others start first whole
+                    int slot = a.hsplit_cap;
+                    if (box > (double)COT_SPLIT_PIX && a.hsplit != nullptr) slot = atomicAdd(a.ovf_count + 13, 1);
+                    if (slot < a.hsplit_cap) a.hsplit[slot] = i;
+                    else a.hlist[atomicAdd(a.ovf_count + 10, 1)] = i;
                     a.cstate[i] = CST_HEAVY;
                 }
             }
@@ -2520,6 +2543,14 @@ __global__ void __launch_bounds__(32 * HEAVY_WARPS, 2) k_cells_heavy(const __gri
     }
 }
 
+// One part of a split cell's integration, out of line so that the rare path
+// leaves the integration kernel's registers to the common one.
+__device__ __noinline__ void integrate_part(FastScratch &S, int nv, const PixGeo pg, double2 si, int lane, int part,
+                                            double *raw)
+{
+    integrate_fast<32, FastScratch, true>(S, nv, pg, si, lane, part, COT_SPLIT, raw);
+}
+
 // The masses and objective terms of the cells whose rings k_cells_fast left
 // in the ring buffer: one warp per cell, fetched from a counter, the same
 // edge-walk integration as the fused path (so the same sums).  Cells above
@@ -2531,19 +2562,63 @@ __global__ void __launch_bounds__(128, MINB) k_integrate(CotGeo g, CellsArgs a)
     FastScratch &S = reinterpret_cast<FastScratch *>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     int *fetch = a.ovf_count + 6;
-    // the heavy list first, then every other cell in order
+    // the parts of the split cells first, then the heavy list, then every
+    // other cell in order
     const int nh = a.hlist != nullptr ? a.ovf_count[10] : 0;
+    const int np = a.hsplit != nullptr ? min(a.ovf_count[13], a.hsplit_cap) * COT_SPLIT : 0;
     while (true) {
         int f = 0;
         if (lane == 0) f = atomicAdd(fetch, 1);
         f = __shfl_sync(FULLMASK, f, 0);
-        if (f >= g.n + nh) break;
+        if (f >= g.n + nh + np) break;
+        if (f < np) {
+            // one part of a split cell: its raw sums to the slot, and the
+            // part that finishes last adds the parts in order
+            const int slot = f / COT_SPLIT, part = f % COT_SPLIT;
+            const int i = a.hsplit[slot];
+            const int nv = a.nv[i];
+            if (lane < nv) {
+                const double2 v = a.rbuf[(size_t)i * COT_RCAP + lane];
+                S.X[lane] = v.x;
+                S.Y[lane] = v.y;
+            }
+            __syncwarp();
+            double raw[6];
+            integrate_part(S, nv, pix_geo(g), g.xy[i], lane, part, raw);
+            if (lane == 0) {
+                double *pp = a.hpart + ((size_t)slot * COT_SPLIT + part) * 4;
+                pp[0] = raw[0];
+                pp[1] = raw[1];
+                pp[2] = raw[2];
+                pp[3] = raw[3];
+                __threadfence();
+                if (atomicAdd(a.hticket + slot, 1u) == COT_SPLIT - 1) {
+                    __threadfence();
+                    const volatile double *q = a.hpart + (size_t)slot * COT_SPLIT * 4;
+                    double sA = q[0], sIa = q[1], sIb = q[2], sI2 = q[3];
+                    for (int k = 1; k < COT_SPLIT; k++) {
+                        sA += q[4 * k];
+                        sIa += q[4 * k + 1];
+                        sIb += q[4 * k + 2];
+                        sI2 += q[4 * k + 3];
+                    }
+                    const double ox = raw[4], oy = raw[5];
+                    const double Sv = sI2 + 2.0 * (ox * sIa + oy * sIb) + (ox * ox + oy * oy) * sA;
+                    a.mu[i] = sA;
+                    a.fc[i] = -(Sv - a.wt[i] * sA);
+                    a.hticket[slot] = 0u;
+                }
+            }
+            __syncwarp();
+            continue;
+        }
+        f -= np;
         int i;
         if (f < nh) {
             i = a.hlist[f];
         } else {
             i = f - nh;
-            if (nh > 0 && a.cstate[i] == CST_HEAVY) continue;
+            if ((nh > 0 || np > 0) && a.cstate[i] == CST_HEAVY) continue;
         }
         const int nv = a.nv[i];
         if (nv > COT_RCAP) continue;
@@ -2920,9 +2995,10 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
     // ovf_count[0..5]: overflow list sizes and fetch counters, [6]: the
     // integration kernel's fetch counter, [8]: k_cells_walk's fetch counter,
     // [9]: k_bucket_walk's, [10]: the heavy integration list's size, [11]:
-    // the overflowed walks' list size, [12]: k_cells_heavy's fetch counter
+    // the overflowed walks' list size, [12]: k_cells_heavy's fetch counter,
+    // [13]: the split integration list's size
     const int segs = (nb * BSEG + 127) / 128;
-    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 13);
+    k_bucket_phi<<<segs, 128, 0, s>>>(g, a.w, a.d, a.tptr, a.wt, a.wbar, a.ovf_count, 14);
     k_tree_build<<<(nb * BSEG + TREE_THREADS - 1) / TREE_THREADS, TREE_THREADS, 0, s>>>(g, a.wt, a.wbar);
     c.launches += 2;
     int upper = 0;  // nodes of levels 1..lmax
@@ -2940,7 +3016,10 @@ void launch_eval(const CotGeo &g, const CellsArgs &args, int cells_per_warp, int
     // the heavy integration list (ovf_list2, which only the 16- and 8-lane
     // paths use otherwise) on the two-kernel path
     a.hlist = (exact || lpc != 32) ? nullptr : a.ovf_list2;
-    if (exact || lpc != 32) a.wlist = nullptr;
+    if (exact || lpc != 32) {
+        a.wlist = nullptr;
+        a.hsplit = nullptr;
+    }
     const int per_sm32 = g_blocks_per_sm32 > 0 ? g_blocks_per_sm32 : CELLS_MINB;
     const int per_sm16 = g_blocks_per_sm16 > 0 ? g_blocks_per_sm16 : CELLS_MINB;
     const int per_sm8 = g_blocks_per_sm8 > 0 ? g_blocks_per_sm8 : 1;

@@ -174,9 +174,18 @@ struct CellsArgs {
     // cells whose certificate walk overflowed its frontier, finished by
     // k_cells_heavy a block each (two-kernel path only; nullable)
     int *wlist;
+    // cells whose integration is shared by several warps (two-kernel path;
+    // nullable): their list (hsplit_cap at most), the parts' raw sums and a
+    // ticket per slot (0 between evaluations)
+    int *hsplit;
+    double *hpart;
+    unsigned int *hticket;
+    int hsplit_cap;
 };
 
 #define COT_HBIG_W 256  // entries of a big Jacobian row (the large-ring pass's capacity)
+#define COT_SPLIT 8          // warps that share the integration of a cell with a very large pixel box
+#define COT_HSPLIT_CAP 2048  // such cells per evaluation (the rest are integrated whole, first)
 
 void launch_eval(const CotGeo &g, const CellsArgs &a, int cells_per_warp, int num_sms,
                  CotCtx &c);
