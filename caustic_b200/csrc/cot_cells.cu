@@ -64,8 +64,16 @@ __shared__ unsigned long long cot_pst[16][16];
 // cell at the last evaluation
 #define COT_NB_HIDDEN 100
 #define COT_RCAP 32  // ring buffer vertices per cell (the split integration)
-#define COT_HEAVY_PIX 1024  // pixel box above which a cell is integrated first
-#define COT_SPLIT_PIX 8192  // pixel box above which a cell is integrated by COT_SPLIT warps
+// pixel box above which a cell is integrated first, and above which by
+// COT_SPLIT warps (measured at 65,536 sites on a 1024^2 target, M cell-evals/s:
+// 512/4096 144.6, 1024/4096 142.5, 512/2048 142.0, 1024/8192 140.8,
+// 1024/16384 139.6, 2048/8192 139.3)
+#ifndef COT_HEAVY_PIX
+#define COT_HEAVY_PIX 512
+#endif
+#ifndef COT_SPLIT_PIX
+#define COT_SPLIT_PIX 4096
+#endif
 #define CST_HEAVY (-2)      // cstate of a cell on the heavy integration list
 
 // ---------------------------------------------------------------------------
