@@ -41,7 +41,7 @@ EXPORTED = [
     "cot_version", "cot_create", "cot_destroy", "cot_set_stream", "cot_set_problem", "cot_eval",
     "cot_cells", "cot_solve", "cot_centroids", "cot_source_masses", "cot_render", "cot_get_kernel_stats",
     "cot_eval_summary_noalloc", "cot_solve_aarl", "cot_source_masses_point_light", "cot_last_error",
-    "cot_set_progress", "cot_solve_batch", "cot_solve_newton", "cot_mass_jacobian",
+    "cot_set_progress", "cot_solve_batch", "cot_solve_newton", "cot_mass_jacobian", "cot_eval_counters",
 ]
 # int (*)(void *user, int phase, int iteration, int status, const double *w, const double *nu, int n,
 #         double grad_norm, double max_rel_err)
@@ -142,6 +142,7 @@ def load():
         L.cot_source_masses_point_light.argtypes = [vp, dp, ctypes.c_int, dp, dp, ctypes.c_double, dp]
         L.cot_render.argtypes = [vp, dp, ctypes.c_double, dp]
         L.cot_get_kernel_stats.argtypes = [vp, ctypes.POINTER(cot_kernel_stats), ctypes.c_int]
+        L.cot_eval_counters.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         L.cot_eval_summary_noalloc.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         L.cot_solve_aarl.argtypes = [vp, vp, ctypes.POINTER(cot_aarl_inputs), ctypes.POINTER(cot_solve_opts),
                                      ctypes.POINTER(cot_solve_stats)]
@@ -277,6 +278,13 @@ class Solver:
         self._check(self._L.cot_get_kernel_stats(self._h, ctypes.byref(st), int(bool(reset))))
         return {"launches": st.launches, "cell_launches": st.cell_launches, "cell_ms": st.cell_ms,
                 "evaluations": st.evaluations}
+
+    def eval_counters(self) -> dict:
+        """Slow paths taken by the last evaluation (cot_eval_counters)."""
+        c = (ctypes.c_int * 4)()
+        self._check(self._L.cot_eval_counters(self._h, c))
+        return {"large_rings": c[0], "walks_by_block": c[1], "integrated_first": c[2],
+                "integrations_split": c[3]}
 
     def set_stream(self, stream_ptr: int):
         self._check(self._L.cot_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

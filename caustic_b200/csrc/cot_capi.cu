@@ -337,6 +337,22 @@ extern "C" int cot_get_kernel_stats(cot_handle *h, cot_kernel_stats *out, int re
     return COT_OK;
 }
 
+extern "C" int cot_eval_counters(cot_handle *h, int *out4)
+{
+    if (!h || !out4) return COT_EINVAL;
+    if (!h->has_problem) return fail(h, COT_ENOPROBLEM, "cot_eval_counters: no problem set", nullptr);
+    COT_CUDA_TRY(cudaSetDevice(h->device));
+    int c[16];
+    COT_CUDA_TRY(cudaMemcpyAsync(c, h->P.ovf_count, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    COT_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    // the counters that the cell kernels fill (cot_cells.cu: launch_eval)
+    out4[0] = c[0];
+    out4[1] = c[11];
+    out4[2] = c[10];
+    out4[3] = std::min(c[13], COT_HSPLIT_CAP);
+    return COT_OK;
+}
+
 extern "C" int cot_last_error(cot_handle *h, char *buf, size_t n)
 {
     const std::string &m = h ? h->err : g_create_err;

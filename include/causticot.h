@@ -352,6 +352,14 @@ COT_API int cot_eval_summary_noalloc(const double *mu, const double *f_cell, con
  * reset=1 clears the counters after reading. */
 COT_API int cot_get_kernel_stats(cot_handle *h, cot_kernel_stats *out, int reset);
 
+/* Which slow paths the last evaluation of this handle took (diagnostics;
+ * no counterpart in the reference): out[0] rings above 32 vertices (the
+ * large-ring pass), out[1] cells whose certificate walk overflowed and was
+ * finished by a block of warps, out[2] cells integrated first because of a
+ * large pixel box, out[3] cells whose integration was shared by several
+ * warps.  Waits for the handle's stream; valid until the next evaluation. */
+COT_API int cot_eval_counters(cot_handle *h, int *out4);
+
 /* Message of the last failure on this handle (or of the last failed
  * cot_create when h is NULL). */
 COT_API int cot_last_error(cot_handle *h, char *buf, size_t n);

@@ -495,3 +495,30 @@ def test_two_cells_per_warp_solve(gpu, cpw):
     for w in (w1, w2):
         assert O.max_rel_error(O.evaluate(oracle_problem(p), w).mu, p.nu) <= 1e-4
     assert np.abs(w1 - w2).max() < 1e-4 * np.abs(w1).max()
+
+
+def test_block_paths_match_oracle(gpu):
+    """The paths that work one cell with several warps, against the oracle.
+    Strongly weighted sites (cells far larger or smaller than their share,
+    as early in a cold solve) give cells whose pixel box is large enough to
+    have their integration started first or shared by several warps; with 2
+    sites per bucket the bound tree is deep enough that certificate walks
+    overflow their frontier, shrink their ring and, when they still
+    overflow, are finished a block each.  Masses, gradient, objective and
+    adjacency as in every evaluation test."""
+    p = problems.make(1, g=64, res=1024)
+    rng = np.random.default_rng(5)
+    seen = {"walks_by_block": 0, "integrations_split": 0, "integrated_first": 0}
+    for bucket_size in (16, 2):
+        s = solver_for(p, bucket_size=bucket_size)
+        for amp in (3.0, 10.0, 30.0):
+            # the first evaluation at new weights: the cached rings of the
+            # last weights mostly fail, as between far trial points
+            w = rng.normal(0.0, amp / p.n, p.n)
+            s.eval(w)
+            c = s.eval_counters()
+            for k in seen:
+                seen[k] += c[k]
+            check_eval(p, w, s)
+        s.close()
+    assert seen["walks_by_block"] > 0 and seen["integrations_split"] > 0 and seen["integrated_first"] > 0, seen
