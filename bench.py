@@ -63,6 +63,8 @@ def parse():
                     help="skip the warm-started arms of the default run")
     ap.add_argument("--warm-steps", type=int, default=0,
                     help="timed solves of each warm-started arm (0: --steps)")
+    ap.add_argument("--no-config5", action="store_true",
+                    help="skip the combined configuration's arms (16 x 262,144 sites, 2048^2)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched configuration's sub-object of the default run")
     return ap.parse_args()
@@ -323,6 +325,67 @@ def batched_arms(args, local, stream):
                                    for c, b, r in tune.table]}}
 
 
+def config5_arms(args, local, workers=8, count=16):
+    """The combined configuration at scale: 16 seeded instances of N = 262,144
+    sites on 2048^2 targets (beam masses), each solved from the host arrays
+    to the same tolerance (i) by the warm pipeline, one instance after
+    another, (ii) by WORKERS warm pipelines side by side (warm.WarmPool: one
+    stream and host thread each), and (iii) cold: the plain L-BFGS from zero
+    on the first instance only (one cold solve takes tens of seconds at this
+    size).  Host wall clock with the device synchronised; the cold solve
+    adds its device time."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+    import torch
+
+    from caustic_b200 import capi, problems
+    from caustic_b200.warm import WarmPool, WarmSolver
+
+    with ThreadPoolExecutor(8) as ex:
+        probs = list(ex.map(lambda i: problems.make(5, i), range(count)))
+    kw = dict(device=local, tol=args.tol, history=args.history)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    with WarmSolver(**kw) as ws:
+        ws.solve(probs[0])                       # warm-up: the handles' buffers
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        seq = [ws.solve(p)[1] for p in probs]
+        torch.cuda.synchronize()
+        seq_s = time.perf_counter() - t0
+    with WarmPool(workers, **kw) as pool:
+        pool.solve_all(probs[:workers])          # warm-up: every pipeline's buffers
+        flush.fill_(2)
+        torch.cuda.synchronize()
+        res, con_s = pool.solve_all(probs)
+        torch.cuda.synchronize()
+    con = [x[1] for x in res]
+    p = probs[0]
+    flush.fill_(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with capi.Solver(device=local) as s:
+        s.set_problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+        _, cst = s.solve(np.zeros(p.n), tol=args.tol, history=args.history, max_iter=100000)
+    cold_wall = time.perf_counter() - t0
+    return {"instances": count, "n_sites": p.n, "image": list(p.size), "masses": "beam_sigma0.35",
+            "warm_sequential_ms_per_solve": 1e3 * seq_s / count,
+            "warm_concurrent_ms_per_solve": 1e3 * con_s / count, "warm_workers": workers,
+            "concurrent_over_sequential": seq_s / con_s,
+            "warm_device_ms_per_solve": float(np.mean([x.device_ms for x in seq])),
+            "warm_converged": all(x.converged for x in seq + con),
+            "warm_max_rel_err": max(x.max_rel_err for x in seq + con),
+            "cold_wall_ms": 1e3 * cold_wall, "cold_device_ms": cst.ms, "cold_iterations": cst.iterations,
+            "cold_evaluations": cst.evaluations, "cold_converged": bool(cst.converged),
+            "cold_max_rel_err": cst.max_rel_err,
+            "cold_cell_evals_per_s": p.n * cst.evaluations / (cst.ms * 1e-3),
+            "speedup_concurrent_wall_vs_cold": cold_wall / (con_s / count),
+            "speedup_sequential_wall_vs_cold": cold_wall / (seq_s / count),
+            "timing": "host wall clock, host arrays in and weights out, device synchronised; the cold arm one "
+                      "instance (the first)"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -496,6 +559,8 @@ def run_ours(args):
                                                  e2e["ms_per_step"] if e2e else None, local)
         if world == 1 and not args.no_batched:
             line["batched_config3"] = batched_arms(args, local, stream)
+        if world == 1 and not args.no_config5:
+            line["config5"] = config5_arms(args, local)
         print(json.dumps(line), flush=True)
     solver.close()
     if dist is not None:

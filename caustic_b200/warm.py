@@ -252,3 +252,65 @@ class WarmSolver:
         w = w.cpu().numpy()
         wall = 1e3 * (time.perf_counter() - t0)
         return w, WarmStats(bool(js.converged), js.max_rel_err, wall, dev_ms, infer_ms, levels, js, lwall, chain_ms)
+
+
+
+class WarmPool:
+    """Warm-started solves of many problems side by side: ``workers``
+    pipelines (each a ``WarmSolver`` with its own stream and handles, kept
+    between calls), each in a host thread of its own, take the problems
+    round robin.  The library calls release the interpreter lock, so the
+    pipelines' many small, latency-bound launches (coarse levels, Newton
+    steps, the judge) overlap on the GPU instead of waiting for one another.
+    Each problem's result is the one ``WarmSolver(**kw).solve`` gives (the
+    same kernels on the same inputs)."""
+
+    def __init__(self, workers: int = 4, **kw):
+        self.solvers = [WarmSolver(**kw) for _ in range(max(1, int(workers)))]
+
+    def close(self):
+        for s in self.solvers:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def solve_all(self, problems):
+        """([(weights, WarmStats)] in problem order, wall seconds of the batch)."""
+        import threading
+
+        import torch
+
+        workers = min(len(self.solvers), len(problems))
+        out = [None] * len(problems)
+        errors = []
+
+        def run(k):
+            try:
+                torch.cuda.set_device(self.solvers[k].device)
+                for i in range(k, len(problems), workers):
+                    out[i] = self.solvers[k].solve(problems[i])
+            except BaseException as e:  # reported on the calling thread
+                errors.append(e)
+
+        t0 = time.perf_counter()
+        threads = [threading.Thread(target=run, args=(k,)) for k in range(workers)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        wall = time.perf_counter() - t0
+        if errors:
+            raise errors[0]
+        return out, wall
+
+
+def solve_concurrent(problems, workers: int = 4, **kw):
+    """One batch through a fresh ``WarmPool`` (its handles are set up inside
+    the timed call).  Returns ([(weights, WarmStats)] in problem order, wall
+    seconds)."""
+    with WarmPool(workers, **kw) as pool:
+        return pool.solve_all(problems)

@@ -54,3 +54,19 @@ def test_learned_start_saves_damped_steps(gpu):
     assert [n for n, _ in sl.levels] == [n for n, _ in sm.levels]
     assert sl.levels[0][1].newton_iterations < sm.levels[0][1].newton_iterations
     assert oracle_err(p, w) <= 1e-4 * (1 + 1e-6)
+
+
+def test_concurrent_pipelines_match_sequential(gpu):
+    """Four problems warm-solved by two pipelines side by side (host threads,
+    one stream each) give the weights of one pipeline solving them in turn,
+    bit for bit, every one converged."""
+    from caustic_b200.warm import solve_concurrent
+
+    ps = [problems.make(2, 20 + i, g=64, res=256) for i in range(4)]
+    with WarmSolver(start="multilevel", min_sites=256) as ws:
+        seq = [ws.solve(p) for p in ps]
+    con, wall = solve_concurrent(ps, workers=2, start="multilevel", min_sites=256)
+    assert wall > 0
+    for (w1, s1), (w2, s2) in zip(seq, con):
+        assert s1.converged and s2.converged and s2.max_rel_err <= 1e-4
+        assert np.array_equal(w1, w2)
