@@ -225,7 +225,9 @@ __device__ __forceinline__ double tree_block_max(double v, double *sh)
 __global__ void __launch_bounds__(TREE_THREADS) k_tree_levels(CotGeo g, const double *__restrict__ wt)
 {
     __shared__ double sh[TREE_THREADS / 32];
-    const int node = g.lev_off[1] + blockIdx.x;
+    // the highest levels (the most sites a node) first, so that they do not
+    // trail the many small nodes of level 1
+    const int node = g.lev_off[1] + (int)(gridDim.x - 1 - blockIdx.x);
     int L = 1;
     while (L + 1 < g.nlev && g.lev_off[L + 1] <= node) L++;
     const int q = node - g.lev_off[L], W = g.lev_w[L];
