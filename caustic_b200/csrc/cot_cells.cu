@@ -35,6 +35,9 @@ namespace cot {
 #define COT_REFINE_PASSES 3  // ring refinements before a walk that overflows scans every bucket
 #define COT_REFINE_ROUNDS 4  // point-location rounds of one refinement
 #define COT_DEFERRED (-3)    // ring size of a cell handed to k_cells_heavy
+#ifndef COT_DEFER_LEAVES
+#define COT_DEFER_LEAVES 24  // surviving leaf buckets above which a walk is handed to k_cells_heavy
+#endif
 #ifndef COT_DEFER_PASS
 #define COT_DEFER_PASS 1  // refinement passes before a walk is handed to k_cells_heavy (1, 2, 3 measured 134.9, 134.8, 134.3 M cell-evals/s: 65,536 sites, 1024² target)
 #endif
@@ -1737,7 +1740,10 @@ __device__ __forceinline__ RegPoly cell_first(const CotGeo &g, const CellsArgs &
         }
         // a hidden cell that reappears gets the window as well, so that
         // the certificate starts from a tight ring
-        if (hidden && P.nv > 0) cached = false;
+#ifndef COT_HIDDEN_WINDOW
+#define COT_HIDDEN_WINDOW 1
+#endif
+        if (COT_HIDDEN_WINDOW && hidden && P.nv > 0) cached = false;
     }
     // the 3x3 buckets around the site: one round of lanes for 16 or 32, two
     // for an 8-lane segment
@@ -1875,6 +1881,23 @@ __device__ __forceinline__ RegPoly cell_walk(const CotGeo &g, const CellsArgs &a
             if (brute) break;
             cur = 1 - cur;
             ncur = nnext;
+        }
+        if constexpr (LPC == 32) {
+            // many surviving leaves: applied in bucket order, their sites
+            // would cost a real clip nearly each; k_cells_heavy tests them
+            // with a block and clips the deepest first
+            if (!brute && ncur > COT_DEFER_LEAVES && a.wlist != nullptr) {
+                if (lane < P.nv) {
+                    a.rbuf[(size_t)i * COT_RCAP + lane] = make_double2(P.x, P.y);
+                    a.lbuf[(size_t)i * COT_RCAP + lane] = P.l;
+                }
+                if (lane == 0) {
+                    a.cstate[i] = P.nv;
+                    a.wlist[atomicAdd(a.ovf_count + 11, 1)] = i;
+                }
+                P.nv = COT_DEFERRED;
+                return P;
+            }
         }
         if (!brute && ncur > 0) {
             // sites of every surviving leaf, LPC leaves at a time
