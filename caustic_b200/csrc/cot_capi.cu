@@ -9,6 +9,7 @@
 #include "cot_common.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -111,7 +112,7 @@ struct cot_handle {
 };
 
 static std::string g_create_err;
-static unsigned long long g_problem_gen = 0;  // problem generations (any handle)
+static std::atomic<unsigned long long> g_problem_gen{0};  // problem generations (any handle, any host thread)
 
 namespace cot {
 
