@@ -20,7 +20,9 @@
 #define COT_MAX_HIST 32
 #define COT_BASIS (2 * COT_MAX_HIST + 1)
 #define COT_NBC 16  // cached neighbours per cell
+#ifndef COT_BLEAF
 #define COT_BLEAF 64 // leaf buckets listed per bucket by the bucket walk (<= the frontier)
+#endif
 
 // Static geometry, passed by value to the kernels.
 struct CotGeo {
