@@ -53,3 +53,42 @@ def test_restriction_keeps_smooth_fields():
     wc = multilevel.restrict(w, fine, coarse)
     ref = 0.3 * coarse.xy[:, 0] - 0.7 * coarse.xy[:, 1]
     assert np.abs(wc - (ref - ref.mean())).max() < 1e-12
+
+
+class _FakeSolver:
+    """Stands in for a pipeline on the host: records which problems it
+    solved, in which thread order, and fails on request."""
+
+    def __init__(self, **kw):
+        self.device = 0
+        self.seen = []
+        self.closed = False
+
+    def solve(self, p):
+        if p == "boom":
+            raise RuntimeError("solve failed")
+        self.seen.append(p)
+        return (p * 10, p)
+
+    def close(self):
+        self.closed = True
+
+
+def test_pool_round_robin_order_and_errors(monkeypatch):
+    """WarmPool hands the problems round robin to its pipelines, returns the
+    results in problem order, closes every pipeline, and raises a pipeline's
+    error on the calling thread."""
+    import torch
+
+    from caustic_b200 import warm
+
+    monkeypatch.setattr(warm, "WarmSolver", _FakeSolver)
+    monkeypatch.setattr(torch.cuda, "set_device", lambda d: None)
+    with warm.WarmPool(3) as pool:
+        out, wall = pool.solve_all(list(range(7)))
+        assert [r[1] for r in out] == list(range(7)) and [r[0] for r in out] == [10 * i for i in range(7)]
+        assert [s.seen for s in pool.solvers] == [[0, 3, 6], [1, 4], [2, 5]]
+        assert wall >= 0.0
+        with pytest.raises(RuntimeError, match="solve failed"):
+            pool.solve_all([1, "boom", 2])
+    assert all(s.closed for s in pool.solvers)
