@@ -671,8 +671,48 @@ def run_warmstart(args):
             "warm_iterations_mean": float(np.mean(res["warm_iters"])),
             "cold_max_rel_err": float(max(res["cold_err"])), "warm_max_rel_err": float(max(res["warm_err"])),
             "clocks": clk.summary()}
+    line["pipelines"] = config4_pipelines(args, probs[:32], path, local)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def config4_pipelines(args, probs, net_path, local):
+    """The same held-out seeds through the warm pipeline (warm.WarmSolver:
+    multilevel damped Newton levels and the plain L-BFGS as the judge), one
+    instance after another, with and without the network's prediction
+    averaged down to the coarsest level as its start, and through the plain
+    L-BFGS from zero one after another (its device time).  Host wall clock
+    per whole solve, host arrays in and weights out."""
+    import numpy as np
+    import torch
+
+    from caustic_b200 import capi, warmstart
+    from caustic_b200.warm import WarmSolver
+
+    out = {"instances": len(probs), "timing": "warm arms: host wall clock per solve; cold: device time per solve"}
+    cold, it = [], []
+    with capi.Solver(device=local) as s:
+        for p in probs:
+            s.set_problem(p.xy, p.nu, p.picture, p.size, p.proj_domain)
+            _, st = s.solve(np.zeros(p.n), tol=args.tol, history=args.history, max_iter=100000)
+            cold.append(st.ms)
+            it.append(st.iterations)
+    out["cold_ms_per_solve"] = float(np.mean(cold))
+    out["cold_iterations_mean"] = float(np.mean(it))
+    net = warmstart.CNet.from_npz(net_path, device=local)   # inference through the C ABI
+    arms = {"multilevel": dict(start="multilevel"),
+            "learned": dict(start="learned", net=net, net_level_sites=probs[0].n, learned_at="coarsest")}
+    for name, kw in arms.items():
+        with WarmSolver(device=local, tol=args.tol, history=args.history, **kw) as ws:
+            ws.solve(probs[0])
+            torch.cuda.synchronize()
+            sts = [ws.solve(p)[1] for p in probs]
+        out[name] = {"wall_ms_per_solve": float(np.mean([x.wall_ms for x in sts])),
+                     "device_ms_per_solve": float(np.mean([x.device_ms for x in sts])),
+                     "converged": all(x.converged for x in sts), "max_rel_err": max(x.max_rel_err for x in sts)}
+    out["learned_over_multilevel"] = out["multilevel"]["wall_ms_per_solve"] / out["learned"]["wall_ms_per_solve"]
+    out["learned_over_cold"] = out["cold_ms_per_solve"] / out["learned"]["wall_ms_per_solve"]
+    return out
 
 
 def run_multilevel(args):
